@@ -1,0 +1,353 @@
+#!/usr/bin/env python
+"""Throughput of the nodal-DG hot path (volume + Rusanov face + LSRK(5,4)
+update) in DOF·stage updates per second.
+
+Default workload: 3-D compressible Euler on the periodic cube [0,2π]^3,
+32^3 hexes at N=7 (16.8 M nodes, 83.9 M DOF), coordinates warped by
+x_i += 0.05 sin x sin y sin z, seeded random Fourier initial state (p = 1),
+dt = 0.2 h / (N^2 max(|u|+c)), FP64.  One "step" is one LSRK(5,4) step
+(5 fused stage launches) over the whole mesh.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--precision 64|32] [--n-side 32] [--order 7]
+
+Under torchrun each rank advances its own copy of the workload (independent
+replicas, "weak" scaling); the timed region is bracketed by a barrier and a
+device synchronisation and the slowest rank's time is reported.
+`--impl reference` times the CPU restatement of the reference's CPU path on
+the host cores instead (rank 0 only).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "canary.jl_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "DOF·stage updates/s"
+
+
+def bytes_per_node(dim, N, w):
+    """Algorithmic HBM bytes per node and stage: Q read+write, residual carry
+    read+write, metric (dim² terms, MJ, MJI) and the face normals + sMJ
+    spread over the nodes (2·dim/Nq face nodes per node)."""
+    ns = 5 if dim == 3 else 4
+    return w * (4 * ns + (dim * dim + 2) + (2.0 * dim / (N + 1)) * (dim + 1))
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic(key):
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f).get(key)
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    FIELDS = ("uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid):
+        self.uuid = uuid
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200",
+                                          "-f", self.path],
+                                         stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        try:
+            with open(self.path) as f:
+                for line in f:
+                    parts = [p.strip() for p in line.split(",")]
+                    if len(parts) < 9:
+                        continue
+                    if self.uuid and self.uuid not in parts[0]:
+                        continue
+                    rows.append(parts)
+            os.unlink(self.path)
+        except Exception:
+            return None
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower().startswith("active")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+def setup_workload(n_side, N, device="cuda", seed=0):
+    from canary_b200 import dg, ic
+    from canary_b200.metric import warp_sinusoidal
+    L = 2 * math.pi
+    mesh = dg.build_mesh(3, N, (np.linspace(0.0, L, n_side + 1),) * 3, (True,) * 3,
+                         meshwarp=lambda X: warp_sinusoidal(X, 0.05))
+    x, y, z = mesh.coords()
+    U, V, W, rho, E = ic.fourier_state(x, y, z, seed=seed, device=device)
+    Q = np.zeros((mesh.Np, 5, mesh.nelem), order="F")
+    Q[:, 0], Q[:, 1], Q[:, 2], Q[:, 3], Q[:, 4] = U, V, W, rho, E
+    dt = ic.fourier_dt(Q, N, h=L / n_side)
+    return mesh, Q, dt
+
+
+def cpu_sample(N, seconds=10.0, n_side=16, max_steps=40):
+    """Oracle (CPU restatement of the reference's CPU path) on a bounded
+    sample of the workload: same N, warp and initial-state law on an
+    n_side^3 mesh, all host threads, LSRK steps until `seconds` elapse."""
+    from canary_b200 import dg
+    from oracle import pyoracle as O
+    mesh, Q, dt = setup_workload(n_side, N, device=None)
+    wp = dict(dg.WORKLOAD_PHYS)
+    wp["lambda"] = wp.pop("lam")
+    phys = O.make_phys(**wp)
+    rhs = np.zeros_like(Q, order="F")
+    cores = os.cpu_count() or 1
+    O.lowstorageRK(3, N, mesh.vgeo, mesh.sgeo, Q, rhs, mesh.D, dt, 1, mesh.vmapM, mesh.vmapP,
+                   mesh.elemtobndy, phys, cores)  # warm-up
+    t0 = time.perf_counter()
+    steps = 0
+    while steps < max_steps and (time.perf_counter() - t0) < seconds:
+        O.lowstorageRK(3, N, mesh.vgeo, mesh.sgeo, Q, rhs, mesh.D, dt, 1, mesh.vmapM, mesh.vmapP,
+                       mesh.elemtobndy, phys, cores)
+        steps += 1
+    el = time.perf_counter() - t0
+    dof = mesh.nelem * mesh.Np * 5
+    return {"value": dof * 5 * steps / el, "unit": METRIC, "cores": cores, "kind": "port",
+            "sample": f"{n_side}^3 hexes N={N} (same warp/IC law), {steps} LSRK steps "
+                      f"({5 * steps} stages) in {el:.1f} s, C oracle with {cores} OpenMP threads"}
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws <= 1:
+        return 0, 1, 0, None
+    import datetime
+    import torch
+    import torch.distributed as tdist
+    rank = int(os.environ["RANK"])
+    local = int(os.environ.get("LOCAL_RANK", rank))
+    torch.cuda.set_device(local)
+    tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                             device_id=torch.device("cuda", local))
+    return rank, ws, local, tdist
+
+
+def run_reference(args, rank):
+    """--impl reference: the CPU path on the host cores (rank 0 only)."""
+    if rank != 0:
+        return
+    from canary_b200 import dg
+    from oracle import pyoracle as O
+    pyoracle_build = O.build
+    pyoracle_build()
+    n_side = args.ref_n_side
+    mesh, Q, dt = setup_workload(n_side, args.order, device=None)
+    wp = dict(dg.WORKLOAD_PHYS)
+    wp["lambda"] = wp.pop("lam")
+    phys = O.make_phys(**wp)
+    rhs = np.zeros_like(Q, order="F")
+    cores = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        O.lowstorageRK(3, args.order, mesh.vgeo, mesh.sgeo, Q, rhs, mesh.D, dt, 1, mesh.vmapM,
+                       mesh.vmapP, mesh.elemtobndy, phys, cores)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        O.lowstorageRK(3, args.order, mesh.vgeo, mesh.sgeo, Q, rhs, mesh.D, dt, 1, mesh.vmapM,
+                       mesh.vmapP, mesh.elemtobndy, phys, cores)
+    el = time.perf_counter() - t0
+    dof = mesh.nelem * mesh.Np * 5
+    val = dof * 5 * args.steps / el
+    line = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": METRIC,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"3-D Euler, periodic [0,2π]^3 warped, N={args.order}, "
+                               f"bounded CPU sample {n_side}^3 hexes of the {args.n_side}^3 workload",
+                   "n_side": n_side, "order": args.order, "dt": dt},
+        "cpu_baseline": {"value": val, "unit": METRIC, "cores": cores, "kind": "port",
+                         "sample": f"{n_side}^3 hexes, N={args.order}, {args.steps} timed LSRK steps; "
+                                   "the reference's Julia CPU path cannot run here (no Julia toolchain), "
+                                   "so its C restatement (oracle/) is timed"},
+        "e2e": {"value": val, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--precision", type=int, default=64, choices=[64, 32])
+    ap.add_argument("--n-side", type=int, default=32)
+    ap.add_argument("--order", type=int, default=7)
+    ap.add_argument("--ref-n-side", type=int, default=8)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    rank, world, local, tdist = dist_init()
+    if args.impl == "reference":
+        run_reference(args, rank)
+        if tdist is not None:
+            tdist.destroy_process_group()
+        return
+
+    import torch
+    from canary_b200 import dg
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    N, dim = args.order, 3
+    mesh, Q, dt = setup_workload(args.n_side, N, device=dev)
+    dm = dg.DeviceMesh.upload(mesh, device=dev)
+    real = torch.float64 if args.precision == 64 else torch.float32
+    dQ = dg.to_device(Q, real, dev)
+    drhs = torch.zeros_like(dQ)
+    solver = dg.LSRK(dm, dQ, drhs, args.precision, dg.make_phys(), stream)
+    dof = mesh.nelem * mesh.Np * 5
+
+    solver.run(args.warmup, dt)
+    torch.cuda.synchronize(dev)
+    try:
+        uuid = str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        uuid = None
+    clocks = ClockSampler(uuid)
+    clocks.start()
+    if tdist is not None:
+        tdist.barrier()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    solver.run(args.steps, dt)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    if tdist is not None:
+        tdist.barrier()
+    clk = clocks.stop()
+    t_ms = e0.elapsed_time(e1)
+    if tdist is not None:
+        tt = torch.tensor([t_ms], dtype=torch.float64, device=dev)
+        tdist.all_reduce(tt, op=tdist.ReduceOp.MAX)
+        t_ms = float(tt.item())
+    sums = solver.sums()
+    finite = bool(np.all(np.isfinite(sums)))
+
+    # end to end through the public API with host buffers: every step copies
+    # the state and residual carry from pinned host memory, advances one
+    # step and reads the state back
+    hQ = torch.empty(dQ.numel(), dtype=real, pin_memory=True)
+    hR = torch.empty(dQ.numel(), dtype=real, pin_memory=True)
+    hQ.copy_(dQ)
+    hR.copy_(drhs)
+    hout = torch.empty_like(hQ, pin_memory=True)
+    torch.cuda.synchronize(dev)
+    if tdist is not None:
+        tdist.barrier()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(args.e2e_steps):
+        dQ.copy_(hQ, non_blocking=True)
+        drhs.copy_(hR, non_blocking=True)
+        solver.run(1, dt)
+        hout.copy_(dQ, non_blocking=True)
+    f1.record(stream)
+    torch.cuda.synchronize(dev)
+    e2e_ms = f0.elapsed_time(f1)
+    if tdist is not None:
+        tt = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+        tdist.all_reduce(tt, op=tdist.ReduceOp.MAX)
+        e2e_ms = float(tt.item())
+    solver.close()
+
+    w = 8 if args.precision == 64 else 4
+    bpn = bytes_per_node(dim, N, w)
+    nodes = mesh.nelem * mesh.Np
+    launches = 5 * args.steps
+    t_launch = t_ms * 1e-3 / launches
+    peak, peak_kind = measured_peaks()
+    achieved = nodes * bpn / t_launch / 1e9
+    key = f"k_stage_3d_N{N}_fp{args.precision}_n{args.n_side}"
+    traffic = load_traffic(key)
+    value = world * dof * 5 * args.steps / (t_ms * 1e-3)
+    bi = 2 * dQ.numel() * w
+    bo = dQ.numel() * w
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == 64 else "f32",
+        "data": "synthetic",
+        "config": {"workload": f"3-D Euler, periodic [0,2π]^3, {args.n_side}^3 hexes, N={N}, "
+                               "warped x_i += 0.05 sin x sin y sin z, seeded Fourier state (seed 0)",
+                   "n_side": args.n_side, "order": N, "nelem": mesh.nelem, "dof": dof, "dt": dt,
+                   "parallelism": f"replicas{world}",
+                   "l2": "inputs larger than L2 (state 0.67 GB, geometry 2.4 GB in FP64)",
+                   "state_finite": finite},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": traffic, "bytes_per_node": bpn, "kernel": "k_stage",
+                     "launch_ms": t_launch * 1e3},
+        "e2e": {"value": world * dof * 5 * args.e2e_steps / (e2e_ms * 1e-3), "unit": METRIC,
+                "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo, "steps": args.e2e_steps},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_sample(N, args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if tdist is not None:
+        tdist.barrier()
+        tdist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

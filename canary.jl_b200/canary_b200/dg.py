@@ -1,0 +1,310 @@
+"""Python mirror of the reference's GPU-method API for the DG hot path.
+
+The reference dispatches `volumerhs!`, `fluxrhs!`, `updatesolution!` and the
+LDG passes on the array type (`rhs::CuArray`, examples/2d_kernels/
+euler2d_set3c.jl:975-996); here the same calls take CUDA torch tensors and
+run the sm_100a kernels of libcanary_b200.so through its C-ABI.  Tensors hold
+the reference's column-major data as flat buffers (a Julia (Np, nstate,
+nelem) array is a C-order (nelem, nstate, Np) tensor), so the memory of a
+`CuArray` and of these tensors is byte-for-byte the same.
+
+Calls are asynchronous on the current torch stream (or `stream=`) and raise
+`CanaryError` on any failure; nothing falls back to a CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from ._lib import CanaryError, cb_phys, check
+from .mesh import brickmesh, connectmesh, mappings, partition
+from .metric import computegeometry
+
+# Physical constants of the reference drivers (euler3d_set3c.jl:113-118,
+# nse2d.jl:127-128): P = (R_gas/c_v)(E - |U|²/2ρ - ρ g z).
+REFERENCE_PHYS = dict(gamma=1.4, R_gas=287.17, c_p=1004.67, c_v=717.5, gravity=10.0,
+                      Pr=7.1, lam=-2.0 / 3.0, visc=0.0)
+# The benchmark workloads: p = (γ-1)(E - ρ|u|²/2) with γ = 1.4, no gravity,
+# nondimensional R = 1 (so R/c_v = γ-1 = 0.4), Pr = 0.72.
+WORKLOAD_PHYS = dict(gamma=1.4, R_gas=1.0, c_p=3.5, c_v=2.5, gravity=0.0, Pr=0.72,
+                     lam=-2.0 / 3.0, visc=0.0)
+
+
+def make_phys(**kw) -> cb_phys:
+    d = dict(WORKLOAD_PHYS)
+    d.update(kw)
+    return cb_phys(d["gamma"], d["R_gas"], d["c_p"], d["c_v"], d["gravity"], d["Pr"],
+                   d["lam"], d["visc"])
+
+
+def nstate(dim: int) -> int:
+    return 5 if dim == 3 else 4
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _ptr(t, dtype, numel=None, name="array"):
+    torch = _torch()
+    if t is None:
+        return None
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError(f"{name} must be a CUDA torch tensor")
+    if t.dtype != dtype:
+        raise TypeError(f"{name} must have dtype {dtype}, got {t.dtype}")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+    if numel is not None and t.numel() < numel:
+        raise ValueError(f"{name} has {t.numel()} entries, needs {numel}")
+    return C.c_void_p(t.data_ptr())
+
+
+def _stream(stream):
+    torch = _torch()
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+def _nelem(elems) -> int:
+    return len(elems) if hasattr(elems, "__len__") else int(elems)
+
+
+def _real(Q):
+    torch = _torch()
+    if Q.dtype == torch.float64:
+        return torch.float64, ""
+    if Q.dtype == torch.float32:
+        return torch.float32, "_f32"
+    raise TypeError("state must be float64 or float32")
+
+
+def _sizes(dim, N, nelem):
+    Nq = N + 1
+    return Nq ** dim, Nq ** (dim - 1), 2 * dim
+
+
+# ---------------------------------------------------------- per-kernel API
+def volumerhs(dim, N, rhs, Q, vgeo, D, elems, phys=None, stream=None):
+    """rhs += volume integral (volumerhs!, euler3d_set3c.jl:253-339)."""
+    torch = _torch()
+    real, suf = _real(Q)
+    n = _nelem(elems)
+    Np, _, _ = _sizes(dim, N, n)
+    ns = nstate(dim)
+    L = _lib.lib()
+    check(getattr(L, "cb_volumerhs" + suf)(
+        dim, N, _ptr(rhs, real, Np * ns * n, "rhs"), _ptr(Q, real, Np * ns * n, "Q"),
+        _ptr(vgeo, real, Np * (14 if dim == 3 else 8) * n, "vgeo"),
+        _ptr(D, real, (N + 1) ** 2, "D"), n, C.byref(phys or make_phys()), _stream(stream)))
+
+
+def fluxrhs(dim, N, rhs, Q, sgeo, vgeo, elems, vmapM, vmapP, elemtobndy, phys=None, stream=None):
+    """rhs -= sMJ · Rusanov flux (fluxrhs!, euler3d_set3c.jl:342-458)."""
+    torch = _torch()
+    real, suf = _real(Q)
+    n = _nelem(elems)
+    Np, Nfp, nf = _sizes(dim, N, n)
+    ns = nstate(dim)
+    L = _lib.lib()
+    check(getattr(L, "cb_fluxrhs" + suf)(
+        dim, N, _ptr(rhs, real, Np * ns * n, "rhs"), _ptr(Q, real, Np * ns * n, "Q"),
+        _ptr(sgeo, real, (dim + 2) * Nfp * nf * n, "sgeo"),
+        _ptr(vgeo, real, Np * (14 if dim == 3 else 8) * n, "vgeo"), n,
+        _ptr(vmapM, torch.int64, Nfp * nf * n, "vmapM"), _ptr(vmapP, torch.int64, Nfp * nf * n, "vmapP"),
+        _ptr(elemtobndy, torch.int64, nf * n, "elemtobndy"), C.byref(phys or make_phys()),
+        _stream(stream)))
+
+
+def updatesolution(dim, N, rhs, rhs_gradQ, Q, vgeo, elems, rka, rkb, dt, visc=0.0, stream=None):
+    """rhs += visc rhs_gradQ[:,:,1,:]; Q += rkb dt rhs MJI; rhs *= rka
+    (updatesolution!, euler3d_set3c.jl:862-872)."""
+    real, suf = _real(Q)
+    n = _nelem(elems)
+    Np, _, _ = _sizes(dim, N, n)
+    ns = nstate(dim)
+    L = _lib.lib()
+    check(getattr(L, "cb_updatesolution" + suf)(
+        dim, N, _ptr(rhs, real, Np * ns * n, "rhs"),
+        _ptr(rhs_gradQ, real, Np * ns * dim * n, "rhs_gradQ") if rhs_gradQ is not None else None,
+        _ptr(Q, real, Np * ns * n, "Q"), _ptr(vgeo, real, None, "vgeo"), n, float(rka), float(rkb),
+        float(dt), float(visc), _stream(stream)))
+
+
+def volume_grad(dim, N, rhs, Q, vgeo, D, elems, phys=None, stream=None):
+    torch = _torch()
+    n = _nelem(elems)
+    check(_lib.lib().cb_volume_grad(dim, N, _ptr(rhs, torch.float64), _ptr(Q, torch.float64),
+                                    _ptr(vgeo, torch.float64), _ptr(D, torch.float64), n,
+                                    C.byref(phys or make_phys()), _stream(stream)))
+
+
+def flux_grad(dim, N, rhs, Q, sgeo, vgeo, elems, vmapM, vmapP, elemtobndy, phys=None, stream=None):
+    torch = _torch()
+    n = _nelem(elems)
+    check(_lib.lib().cb_flux_grad(dim, N, _ptr(rhs, torch.float64), _ptr(Q, torch.float64),
+                                  _ptr(sgeo, torch.float64), _ptr(vgeo, torch.float64), n,
+                                  _ptr(vmapM, torch.int64), _ptr(vmapP, torch.int64),
+                                  _ptr(elemtobndy, torch.int64), C.byref(phys or make_phys()),
+                                  _stream(stream)))
+
+
+def update_gradQ(dim, N, gradQ, rhs, vgeo, elems, stream=None):
+    torch = _torch()
+    n = _nelem(elems)
+    check(_lib.lib().cb_update_gradQ(dim, N, _ptr(gradQ, torch.float64), _ptr(rhs, torch.float64),
+                                     _ptr(vgeo, torch.float64), n, _stream(stream)))
+
+
+def volume_div(dim, N, rhs, gradQ, Q, vgeo, D, elems, phys=None, stream=None):
+    torch = _torch()
+    n = _nelem(elems)
+    check(_lib.lib().cb_volume_div(dim, N, _ptr(rhs, torch.float64), _ptr(gradQ, torch.float64),
+                                   _ptr(Q, torch.float64), _ptr(vgeo, torch.float64),
+                                   _ptr(D, torch.float64), n, C.byref(phys or make_phys()),
+                                   _stream(stream)))
+
+
+def flux_div(dim, N, rhs, gradQ, Q, sgeo, elems, vmapM, vmapP, elemtobndy, phys=None, stream=None):
+    torch = _torch()
+    n = _nelem(elems)
+    check(_lib.lib().cb_flux_div(dim, N, _ptr(rhs, torch.float64), _ptr(gradQ, torch.float64),
+                                 _ptr(Q, torch.float64), _ptr(sgeo, torch.float64), n,
+                                 _ptr(vmapM, torch.int64), _ptr(vmapP, torch.int64),
+                                 _ptr(elemtobndy, torch.int64), C.byref(phys or make_phys()),
+                                 _stream(stream)))
+
+
+def device_status(stream=None) -> None:
+    """Synchronise and raise if a kernel met an invalid boundary code or a
+    non-finite state since the last check."""
+    check(_lib.lib().cb_device_status(_stream(stream)))
+
+
+# ------------------------------------------------------------------ mesh
+@dataclass
+class Mesh:
+    """Host-side mesh data of one DG instance, reference layouts (numpy)."""
+    dim: int
+    N: int
+    nelem: int
+    vgeo: np.ndarray
+    sgeo: np.ndarray
+    vmapM: np.ndarray
+    vmapP: np.ndarray
+    elemtobndy: np.ndarray
+    D: np.ndarray
+    r: np.ndarray
+    w: np.ndarray
+    elemtocoord: np.ndarray
+
+    @property
+    def Np(self):
+        return (self.N + 1) ** self.dim
+
+    def coords(self):
+        nm = self.dim * self.dim
+        return tuple(self.vgeo[:, nm + 2 + c, :] for c in range(self.dim))
+
+
+def build_mesh(dim, N, x, periodic, boundary=None, meshwarp=None) -> Mesh:
+    """brickmesh -> partition -> connectmesh -> mappings -> computegeometry,
+    the setup sequence of euler() (euler3d_set3c.jl:1689-1708)."""
+    cm = connectmesh(*partition(*brickmesh(x, periodic, boundary=boundary)))
+    vmapM, vmapP = mappings(N, cm["elemtoelem"], cm["elemtoface"], cm["elemtoordr"])
+    vgeo, sgeo, r, w, D = computegeometry(dim, N, cm["elemtocoord"], vmapM, meshwarp)
+    return Mesh(dim, N, vgeo.shape[2], vgeo, sgeo, vmapM, vmapP, cm["elemtobndy"], D, r, w,
+                cm["elemtocoord"])
+
+
+def to_device(a: np.ndarray, dtype=None, device="cuda"):
+    """Column-major numpy array -> flat CUDA tensor with the same memory order."""
+    torch = _torch()
+    flat = np.asarray(a).ravel(order="F")
+    t = torch.from_numpy(np.ascontiguousarray(flat))
+    if dtype is not None:
+        t = t.to(dtype)
+    return t.to(device)
+
+
+def from_device(t, shape) -> np.ndarray:
+    """Flat tensor -> Fortran-ordered numpy array of the Julia shape."""
+    return np.asarray(t.detach().cpu().numpy()).reshape(shape, order="F")
+
+
+@dataclass
+class DeviceMesh:
+    """Device copies of one mesh (FP64 geometry, int64 maps)."""
+    mesh: Mesh
+    vgeo: object
+    sgeo: object
+    vmapM: object
+    vmapP: object
+    elemtobndy: object
+    D: object
+
+    @classmethod
+    def upload(cls, mesh: Mesh, device="cuda"):
+        torch = _torch()
+        return cls(mesh, to_device(mesh.vgeo, torch.float64, device), to_device(mesh.sgeo, torch.float64, device),
+                   to_device(mesh.vmapM, torch.int64, device), to_device(mesh.vmapP, torch.int64, device),
+                   to_device(mesh.elemtobndy, torch.int64, device), to_device(mesh.D, torch.float64, device))
+
+
+# ---------------------------------------------------------------- solver
+class LSRK:
+    """Fused, graph-captured LSRK(5,4) driver bound to one state (the
+    lowstorageRK of euler3d_set3c.jl:1361-1523 / nse2d.jl:1728-1890).
+
+    Q and rhs are CUDA tensors owned by the caller (float64 for precision 64,
+    float32 for precision 32); they are advanced in place."""
+
+    def __init__(self, dmesh: DeviceMesh, Q, rhs, precision=64, phys=None, stream=None):
+        torch = _torch()
+        m = dmesh.mesh
+        real = torch.float64 if precision == 64 else torch.float32
+        n = m.nelem * m.Np * nstate(m.dim)
+        self.dmesh, self.Q, self.rhs, self.precision = dmesh, Q, rhs, precision
+        self.phys = phys or make_phys()
+        self._h = C.c_void_p()
+        self._stream = stream
+        check(_lib.lib().cb_solver_create(
+            C.byref(self._h), m.dim, m.N, precision, m.nelem, _ptr(Q, real, n, "Q"),
+            _ptr(rhs, real, n, "rhs"), _ptr(dmesh.vgeo, torch.float64), _ptr(dmesh.sgeo, torch.float64),
+            _ptr(dmesh.vmapM, torch.int64), _ptr(dmesh.vmapP, torch.int64),
+            _ptr(dmesh.elemtobndy, torch.int64), _ptr(dmesh.D, torch.float64),
+            C.byref(self.phys), _stream(stream)))
+
+    def run(self, nsteps: int, dt: float) -> None:
+        check(_lib.lib().cb_lsrk_run(self._h, int(nsteps), float(dt)))
+
+    def sums(self) -> np.ndarray:
+        """Compensated FP64 (Σ MJ Q_s, Σ MJ Q_s²) per field, shape (2, nstate)."""
+        ns = nstate(self.dmesh.mesh.dim)
+        out = (C.c_double * (2 * ns))()
+        check(_lib.lib().cb_solver_sums(self._h, out))
+        return np.array(out[:]).reshape(2, ns)
+
+    def close(self) -> None:
+        if self._h:
+            _lib.lib().cb_solver_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def lowstorageRK(dim, N, dmesh: DeviceMesh, Q, rhs, dt, nsteps, precision=64, phys=None, stream=None):
+    """Advance Q (and the residual carry rhs) by nsteps LSRK(5,4) steps."""
+    s = LSRK(dmesh, Q, rhs, precision, phys, stream)
+    try:
+        s.run(nsteps, dt)
+    finally:
+        s.close()

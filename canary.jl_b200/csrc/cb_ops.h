@@ -1,0 +1,41 @@
+// Host-side table of launchers for one (dim, precision, order).
+#pragma once
+#include "cb_dg.cuh"
+
+namespace cb {
+
+constexpr int MAXN = 10;  // orders 1..MAXN are compiled for dim 2 and 3
+
+template <typename T>
+struct Ops {
+  int Np, Nfp, epb, threads;
+  size_t smem_stage;
+  // sets the dynamic shared-memory limits of every kernel of this order
+  cudaError_t (*prepare)();
+  cudaError_t (*volumerhs)(T *, const T *, const T *, const T *, int64_t, const PhysT<T> &, cudaStream_t);
+  cudaError_t (*fluxrhs)(T *, const T *, const T *, const T *, int64_t, const int64_t *,
+                         const int64_t *, const int64_t *, const PhysT<T> &, unsigned *, cudaStream_t);
+  cudaError_t (*stage)(const T *, T *, T *, const T *, const T *, const int32_t *, const T *, int64_t,
+                       const PhysT<T> &, T, T, unsigned *, cudaStream_t);
+  cudaError_t (*build_nbr)(int32_t *, const int64_t *, const int64_t *, const int64_t *, int64_t,
+                           unsigned *, cudaStream_t);
+  cudaError_t (*volume_grad)(T *, const T *, const T *, const T *, int64_t, const PhysT<T> &, cudaStream_t);
+  cudaError_t (*flux_grad)(T *, const T *, const T *, const T *, int64_t, const int64_t *,
+                           const int64_t *, const int64_t *, const PhysT<T> &, unsigned *, cudaStream_t);
+  cudaError_t (*volume_div)(T *, const T *, const T *, const T *, const T *, int64_t, const PhysT<T> &,
+                            cudaStream_t);
+  cudaError_t (*flux_div)(T *, const T *, const T *, const T *, int64_t, const int64_t *, const int64_t *,
+                          const int64_t *, const PhysT<T> &, unsigned *, cudaStream_t);
+  // order-independent element-wise kernels
+  cudaError_t (*update)(T *, const T *, T *, const T *, int64_t, int, T, T, T, T, cudaStream_t);
+  cudaError_t (*update_gradQ)(T *, const T *, const T *, int64_t, int, cudaStream_t);
+  cudaError_t (*cons_sums)(const T *, const T *, int64_t, int, double *, int, cudaStream_t);
+};
+
+// Defined in cb_inst_<dim>d_<prec>.cu; nullptr when N is outside 1..MAXN.
+template <int DIM, typename T>
+const Ops<T> *get_ops(int N);
+
+cudaError_t round_to_f32(float *dst, const double *src, int64_t n, cudaStream_t st);
+
+}  // namespace cb

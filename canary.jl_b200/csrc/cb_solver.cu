@@ -1,0 +1,301 @@
+// Fused, graph-captured LSRK(5,4) solver behind cb_solver_* / cb_lsrk_run.
+//
+// Inviscid form: one k_stage launch per RK stage reads Q from one buffer and
+// writes the next state into the other (neighbour traces must see the state
+// at the start of the stage), so the state ping-pongs between the caller's Q
+// and a solver-owned twin.  Two steps (ten stages) return to the caller's
+// buffer and are captured as one CUDA graph; an odd final step is launched
+// directly and copied back.
+// Viscous (LDG Navier–Stokes) form: the reference sequence of passes per
+// stage (volume, face, gradient, divergence, update) on a single buffer,
+// captured one step per graph.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+
+#include "../../include/canary_b200.h"
+#include "cb_ops.h"
+
+using namespace cb;
+
+namespace cb {
+int solver_fail(int code, const char *fmt, ...);
+}
+
+struct cb_solver {
+  int dim = 0, N = 0, prec = 64, device = 0;
+  int64_t nelem = 0;
+  void *Q = nullptr, *rhs = nullptr, *Qalt = nullptr;
+  const void *vgeo = nullptr, *sgeo = nullptr, *D = nullptr;
+  void *owned_geo = nullptr;  // FP32 copies of vgeo | sgeo | D (precision 32)
+  const int64_t *vmapM = nullptr, *vmapP = nullptr, *bnd = nullptr;
+  int32_t *nbr = nullptr;
+  void *gradQ = nullptr, *rhs_gradQ = nullptr;
+  cb_phys phys{};
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  unsigned *status = nullptr;
+  double *part = nullptr;
+  int part_blocks = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  double graph_dt = NAN;
+};
+
+namespace {
+
+const double RKA[5] = {0.0, -567301805773.0 / 1357537059087.0, -2404267990393.0 / 2016746695238.0,
+                       -3550918686646.0 / 2091501179385.0, -1275806237668.0 / 842570457699.0};
+const double RKB[5] = {1432997174477.0 / 9575080441755.0, 5161836677717.0 / 13612068292357.0,
+                       1720146321549.0 / 2090206949498.0, 3134564353537.0 / 4481467310338.0,
+                       2277821191437.0 / 14882151754819.0};
+
+template <typename T>
+const Ops<T> *ops(const cb_solver *s) {
+  return s->dim == 2 ? get_ops<2, T>(s->N) : get_ops<3, T>(s->N);
+}
+
+template <typename T>
+cudaError_t enqueue_step(cb_solver *s, double dt, bool from_user) {
+  const Ops<T> *o = ops<T>(s);
+  const PhysT<T> p(Phys{s->phys.gamma, s->phys.R_gas, s->phys.c_p, s->phys.c_v, s->phys.gravity,
+                        s->phys.Pr, s->phys.lambda, s->phys.visc});
+  const T *vg = (const T *)s->vgeo, *sg = (const T *)s->sgeo, *D = (const T *)s->D;
+  cudaError_t e = cudaSuccess;
+  if (s->phys.visc > 0) {
+    T *Q = (T *)s->Q, *rhs = (T *)s->rhs, *gQ = (T *)s->gradQ, *rg = (T *)s->rhs_gradQ;
+    for (int st = 0; st < 5 && e == cudaSuccess; ++st) {
+      if ((e = o->volumerhs(rhs, Q, vg, D, s->nelem, p, s->stream)) != cudaSuccess) break;
+      if ((e = o->fluxrhs(rhs, Q, sg, vg, s->nelem, s->vmapM, s->vmapP, s->bnd, p, s->status, s->stream)) != cudaSuccess) break;
+      if ((e = o->volume_grad(rg, Q, vg, D, s->nelem, p, s->stream)) != cudaSuccess) break;
+      if ((e = o->flux_grad(rg, Q, sg, vg, s->nelem, s->vmapM, s->vmapP, s->bnd, p, s->status, s->stream)) != cudaSuccess) break;
+      if ((e = o->update_gradQ(gQ, rg, vg, s->nelem, o->Np, s->stream)) != cudaSuccess) break;
+      if ((e = o->volume_div(rg, gQ, Q, vg, D, s->nelem, p, s->stream)) != cudaSuccess) break;
+      if ((e = o->flux_div(rg, gQ, Q, sg, s->nelem, s->vmapM, s->vmapP, s->bnd, p, s->status, s->stream)) != cudaSuccess) break;
+      e = o->update(rhs, rg, Q, vg, s->nelem, o->Np, T(RKA[(st + 1) % 5]), T(RKB[st]), T(dt), T(s->phys.visc), s->stream);
+    }
+    return e;
+  }
+  T *a = (T *)(from_user ? s->Q : s->Qalt), *b = (T *)(from_user ? s->Qalt : s->Q);
+  for (int st = 0; st < 5 && e == cudaSuccess; ++st) {
+    e = o->stage(a, b, (T *)s->rhs, vg, sg, s->nbr, D, s->nelem, p, T(RKA[(st + 1) % 5]),
+                 T(RKB[st] * dt), s->status, s->stream);
+    T *t = a;
+    a = b;
+    b = t;
+  }
+  return e;
+}
+
+cudaError_t enqueue(cb_solver *s, double dt, bool from_user) {
+  return s->prec == 64 ? enqueue_step<double>(s, dt, from_user) : enqueue_step<float>(s, dt, from_user);
+}
+
+void drop_graph(cb_solver *s) {
+  if (s->exec) cudaGraphExecDestroy(s->exec);
+  if (s->graph) cudaGraphDestroy(s->graph);
+  s->exec = nullptr;
+  s->graph = nullptr;
+  s->graph_dt = NAN;
+}
+
+int capture(cb_solver *s, double dt) {
+  drop_graph(s);
+  cudaError_t e = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return solver_fail(CB_ERR_CUDA, "begin capture: %s", cudaGetErrorString(e));
+  cudaError_t e1 = enqueue(s, dt, true);
+  if (s->phys.visc <= 0 && e1 == cudaSuccess) e1 = enqueue(s, dt, false);  // two steps
+  e = cudaStreamEndCapture(s->stream, &s->graph);
+  if (e1 != cudaSuccess || e != cudaSuccess) {
+    drop_graph(s);
+    return solver_fail(CB_ERR_CUDA, "capture: %s", cudaGetErrorString(e1 != cudaSuccess ? e1 : e));
+  }
+  e = cudaGraphInstantiate(&s->exec, s->graph, 0);
+  if (e != cudaSuccess) {
+    drop_graph(s);
+    return solver_fail(CB_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+  }
+  s->graph_dt = dt;
+  return CB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cb_solver_create(cb_solver **out, int dim, int N, int precision, int64_t nelem, void *Q,
+                     void *rhs, const double *vgeo, const double *sgeo, const int64_t *vmapM,
+                     const int64_t *vmapP, const int64_t *elemtobndy, const double *D,
+                     const cb_phys *phys, cb_stream_t stream) {
+  if (!out || !Q || !rhs || !vgeo || !sgeo || !vmapM || !vmapP || !elemtobndy || !D || !phys)
+    return solver_fail(CB_ERR_ARG, "cb_solver_create: null pointer argument");
+  if (dim != 2 && dim != 3) return solver_fail(CB_ERR_ARG, "dim must be 2 or 3");
+  if (precision != 32 && precision != 64) return solver_fail(CB_ERR_ARG, "precision must be 32 or 64");
+  if (nelem <= 0) return solver_fail(CB_ERR_ARG, "nelem must be positive");
+  if (N < 1 || N > MAXN) return solver_fail(CB_ERR_UNSUPPORTED, "order N=%d outside 1..%d", N, MAXN);
+  *out = nullptr;
+  cb_solver *s = new cb_solver();
+  s->dim = dim;
+  s->N = N;
+  s->prec = precision;
+  s->nelem = nelem;
+  s->Q = Q;
+  s->rhs = rhs;
+  s->vmapM = vmapM;
+  s->vmapP = vmapP;
+  s->bnd = elemtobndy;
+  s->phys = *phys;
+  cudaGetDevice(&s->device);
+  const int Nq = N + 1;
+  const int64_t Np = dim == 2 ? (int64_t)Nq * Nq : (int64_t)Nq * Nq * Nq;
+  const int64_t Nfp = dim == 2 ? Nq : (int64_t)Nq * Nq;
+  const int ns = dim == 2 ? 4 : 5, nvg = dim == 2 ? 8 : 14, nsg = dim == 2 ? 4 : 5, nface = 2 * dim;
+  const size_t w = precision == 64 ? 8 : 4;
+  cudaError_t e = cudaSuccess;
+  auto bail = [&](int code, const char *what) {
+    cb_solver_destroy(s);
+    return solver_fail(code, "cb_solver_create: %s: %s", what, cudaGetErrorString(e));
+  };
+  if (stream) {
+    s->stream = (cudaStream_t)stream;
+  } else {
+    // graph capture is not allowed on the legacy default stream; a blocking
+    // stream stays ordered with work the caller put on stream 0
+    if ((e = cudaStreamCreate(&s->stream)) != cudaSuccess) return bail(CB_ERR_CUDA, "stream");
+    s->own_stream = true;
+  }
+  if ((e = cudaMalloc(&s->status, sizeof(unsigned))) != cudaSuccess) return bail(CB_ERR_NOMEM, "status");
+  cudaMemsetAsync(s->status, 0, sizeof(unsigned), s->stream);
+  s->part_blocks = 296;
+  if ((e = cudaMalloc(&s->part, sizeof(double) * 4 * ns * s->part_blocks)) != cudaSuccess)
+    return bail(CB_ERR_NOMEM, "partials");
+  if (phys->visc > 0) {
+    const size_t gbytes = w * (size_t)Np * ns * dim * nelem;
+    if ((e = cudaMalloc(&s->gradQ, gbytes)) != cudaSuccess) return bail(CB_ERR_NOMEM, "gradQ");
+    if ((e = cudaMalloc(&s->rhs_gradQ, gbytes)) != cudaSuccess) return bail(CB_ERR_NOMEM, "rhs_gradQ");
+    cudaMemsetAsync(s->gradQ, 0, gbytes, s->stream);
+    cudaMemsetAsync(s->rhs_gradQ, 0, gbytes, s->stream);
+  } else {
+    if ((e = cudaMalloc(&s->Qalt, w * (size_t)Np * ns * nelem)) != cudaSuccess) return bail(CB_ERR_NOMEM, "state twin");
+    if ((e = cudaMalloc(&s->nbr, sizeof(int32_t) * nface * nelem)) != cudaSuccess) return bail(CB_ERR_NOMEM, "neighbours");
+  }
+  if (precision == 64) {
+    s->vgeo = vgeo;
+    s->sgeo = sgeo;
+    s->D = D;
+  } else {
+    const int64_t nv = Np * nvg * nelem, ns_ = nsg * Nfp * nface * nelem, nd = (int64_t)Nq * Nq;
+    if ((e = cudaMalloc(&s->owned_geo, sizeof(float) * (nv + ns_ + nd))) != cudaSuccess)
+      return bail(CB_ERR_NOMEM, "fp32 geometry");
+    float *g = (float *)s->owned_geo;
+    round_to_f32(g, vgeo, nv, s->stream);
+    round_to_f32(g + nv, sgeo, ns_, s->stream);
+    round_to_f32(g + nv + ns_, D, nd, s->stream);
+    s->vgeo = g;
+    s->sgeo = g + nv;
+    s->D = g + nv + ns_;
+  }
+  e = precision == 64 ? ops<double>(s)->prepare() : ops<float>(s)->prepare();
+  if (e != cudaSuccess) return bail(CB_ERR_CUDA, "kernel attributes");
+  if (phys->visc <= 0) {
+    const Ops<double> *o = ops<double>(s);
+    if ((e = o->build_nbr(s->nbr, vmapM, vmapP, elemtobndy, nelem, s->status, s->stream)) != cudaSuccess)
+      return bail(CB_ERR_CUDA, "neighbour table");
+  }
+  unsigned h = 0;
+  if ((e = cudaMemcpyAsync(&h, s->status, sizeof h, cudaMemcpyDeviceToHost, s->stream)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(s->stream)) != cudaSuccess)
+    return bail(CB_ERR_CUDA, "setup");
+  if (h & ST_BC) {
+    cb_solver_destroy(s);
+    return solver_fail(CB_ERR_BC, "invalid boundary condition code (only 0 and 1 are defined)");
+  }
+  if (h & ST_MESH) {
+    cb_solver_destroy(s);
+    return solver_fail(CB_ERR_MESH, "vmapM/vmapP do not describe a conforming mesh with orientation 1");
+  }
+  *out = s;
+  return CB_OK;
+}
+
+int cb_lsrk_run(cb_solver *s, int64_t nsteps, double dt) {
+  if (!s) return solver_fail(CB_ERR_ARG, "null solver");
+  if (nsteps < 0) return solver_fail(CB_ERR_ARG, "nsteps must be >= 0");
+  if (nsteps == 0) return CB_OK;
+  const int64_t per_graph = s->phys.visc > 0 ? 1 : 2;
+  const int64_t reps = nsteps / per_graph, rem = nsteps % per_graph;
+  cudaError_t e;
+  if (reps > 0) {
+    if (!s->exec || s->graph_dt != dt) {
+      int rc = capture(s, dt);
+      if (rc) return rc;
+    }
+    for (int64_t r = 0; r < reps; ++r)
+      if ((e = cudaGraphLaunch(s->exec, s->stream)) != cudaSuccess)
+        return solver_fail(CB_ERR_CUDA, "graph launch: %s", cudaGetErrorString(e));
+  }
+  if (rem) {
+    if ((e = enqueue(s, dt, true)) != cudaSuccess)
+      return solver_fail(CB_ERR_CUDA, "step launch: %s", cudaGetErrorString(e));
+    const int Nq = s->N + 1;
+    const int64_t Np = s->dim == 2 ? (int64_t)Nq * Nq : (int64_t)Nq * Nq * Nq;
+    const size_t bytes = (s->prec == 64 ? 8 : 4) * (size_t)Np * (s->dim == 2 ? 4 : 5) * s->nelem;
+    if ((e = cudaMemcpyAsync(s->Q, s->Qalt, bytes, cudaMemcpyDeviceToDevice, s->stream)) != cudaSuccess)
+      return solver_fail(CB_ERR_CUDA, "state copy: %s", cudaGetErrorString(e));
+  }
+  return CB_OK;
+}
+
+int cb_solver_sums(cb_solver *s, double *out_host) {
+  if (!s || !out_host) return solver_fail(CB_ERR_ARG, "null argument");
+  const int ns = s->dim == 2 ? 4 : 5, Nq = s->N + 1;
+  const int Np = s->dim == 2 ? Nq * Nq : Nq * Nq * Nq;
+  cudaError_t e = s->prec == 64
+                      ? ops<double>(s)->cons_sums((const double *)s->Q, (const double *)s->vgeo, s->nelem, Np, s->part, s->part_blocks, s->stream)
+                      : ops<float>(s)->cons_sums((const float *)s->Q, (const float *)s->vgeo, s->nelem, Np, s->part, s->part_blocks, s->stream);
+  if (e != cudaSuccess) return solver_fail(CB_ERR_CUDA, "sums launch: %s", cudaGetErrorString(e));
+  std::string buf(sizeof(double) * 4 * ns * s->part_blocks, '\0');
+  double *h = (double *)&buf[0];
+  unsigned st = 0;
+  if ((e = cudaMemcpyAsync(h, s->part, buf.size(), cudaMemcpyDeviceToHost, s->stream)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(&st, s->status, sizeof st, cudaMemcpyDeviceToHost, s->stream)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(s->stream)) != cudaSuccess)
+    return solver_fail(CB_ERR_CUDA, "sums: %s", cudaGetErrorString(e));
+  for (int q = 0; q < 2 * ns; ++q) {
+    double sum = 0.0, comp = 0.0;
+    for (int b = 0; b < s->part_blocks; ++b) {
+      const double v = h[b * 4 * ns + 2 * q], c = h[b * 4 * ns + 2 * q + 1];
+      const double t = sum + v;
+      if (std::fabs(sum) >= std::fabs(v)) comp += (sum - t) + v;
+      else comp += (v - t) + sum;
+      sum = t;
+      comp += c;
+    }
+    // q = 2*s + k  (k = 0: Σ MJ Q, k = 1: Σ MJ Q²) -> out[k*ns + s]
+    out_host[(q % 2) * ns + q / 2] = sum + comp;
+  }
+  if (st & ST_NONFINITE) return solver_fail(CB_ERR_NONFINITE, "the state became non-finite");
+  if (st & ST_BC) return solver_fail(CB_ERR_BC, "invalid boundary condition code");
+  return CB_OK;
+}
+
+int cb_solver_destroy(cb_solver *s) {
+  if (!s) return CB_OK;
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  drop_graph(s);
+  cudaFree(s->Qalt);
+  cudaFree(s->nbr);
+  cudaFree(s->gradQ);
+  cudaFree(s->rhs_gradQ);
+  cudaFree(s->owned_geo);
+  cudaFree(s->status);
+  cudaFree(s->part);
+  if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+  return CB_OK;
+}
+
+}  // extern "C"

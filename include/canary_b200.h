@@ -1,0 +1,181 @@
+/*
+ * canary_b200 — C-ABI of the B200 (sm_100a) nodal-DG hot path of
+ * CliMA/Canary.jl: volume RHS, Rusanov face flux, LDG Navier–Stokes passes
+ * and the Carpenter–Kennedy LSRK(5,4) update.
+ *
+ * Every array argument is a DEVICE pointer owned by the caller and uses the
+ * reference's column-major Julia layout unchanged:
+ *
+ *   Q, rhs       (Np, nstate, nelem)          state order 3-D (U,V,W,ρ,E),
+ *                                              2-D (U,V,ρ,E)
+ *   gradQ        (Np, nstate, dim, nelem)
+ *   vgeo         (Np, nvgeo, nelem)           3-D (ξx,ηx,ζx,ξy,ηy,ζy,ξz,ηz,ζz,
+ *                                              MJ,MJI,x,y,z); 2-D (ξx,ηx,ξy,ηy,
+ *                                              MJ,MJI,x,y)
+ *   sgeo         (nsgeo, Nfp, nface, nelem)   3-D (nx,ny,nz,sMJ,vMJI);
+ *                                              2-D (nx,ny,sMJ,vMJI)
+ *   vmapM/vmapP  (Nfp, nface, nelem) int64, 1-based node ids (mesh.jl:973)
+ *   elemtobndy   (nface, nelem) int64, 0 = connected face, 1 = wall
+ *   D            (Nq, Nq) spectral derivative matrix (operators.jl:84)
+ *
+ * with Nq = N+1, Np = Nq^dim, Nfp = Nq^(dim-1), nface = 2 dim.  Calls are
+ * asynchronous on `stream` (0 = legacy default stream) and return a status
+ * code; they never synchronise the device except where stated.
+ *
+ * The `_f32` twins take single-precision arrays of the same layouts.
+ */
+#ifndef CANARY_B200_H
+#define CANARY_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st *cb_stream_t; /* == cudaStream_t */
+
+/* Status codes. */
+enum {
+  CB_OK = 0,
+  CB_ERR_ARG = 1,         /* bad dimension, order, size or null pointer   */
+  CB_ERR_UNSUPPORTED = 2, /* (dim, N) outside the compiled range          */
+  CB_ERR_BC = 3,          /* boundary code other than 0 or 1              */
+  CB_ERR_CUDA = 4,        /* a CUDA runtime call failed                   */
+  CB_ERR_MESH = 5,        /* vmapM/vmapP do not describe a conforming mesh*/
+  CB_ERR_NONFINITE = 6,   /* the state became NaN or Inf                  */
+  CB_ERR_TIMEOUT = 7,     /* a bounded device wait gave up                */
+  CB_ERR_NOMEM = 8        /* allocation failed                            */
+};
+
+/* Physical constants of the set3c / nse formulations.  Reference values:
+ * euler3d_set3c.jl:113-118 (γ=7/5, R_gas=287.17, c_p=1004.67, c_v=717.5,
+ * gravity=10) and nse2d.jl:127-128 (Pr=71/10, λ=-2/3).  The pressure law is
+ * P = (R_gas/c_v)(E - |U|²/(2ρ) - ρ g x_dim); `visc` multiplies the viscous
+ * residual as the `visc` argument of nse()/updatesolution! does. */
+typedef struct cb_phys {
+  double gamma;
+  double R_gas;
+  double c_p;
+  double c_v;
+  double gravity;
+  double Pr;
+  double lambda;
+  double visc;
+} cb_phys;
+
+/* Library identification and error reporting. */
+int cb_version(void);
+/* Message of the last failing call on this host thread ("" if none). */
+const char *cb_last_error(void);
+/* Synchronises `stream` and returns (and clears) the sticky device-side
+ * status raised by kernels since the last call: CB_ERR_BC when a face with a
+ * boundary code other than 0/1 was met (that face is skipped, as no valid
+ * flux exists), CB_ERR_NONFINITE, or CB_OK. */
+int cb_device_status(cb_stream_t stream);
+/* Largest polynomial order compiled for `dim` (orders 1..max are built). */
+int cb_max_order(int dim);
+
+/* ---------------------------------------------------------------------- */
+/* Per-function drop-ins of the reference's kernels (stateless).          */
+/* ---------------------------------------------------------------------- */
+
+/* rhs += volume integral (and the -MJ ρ g buoyancy source).
+ * Replaces volumerhs!(Val(dim), Val(N), d_rhsC::CuArray, d_QC, d_vgeoC, d_D,
+ * elems): euler2d_set3c.jl:975-980 / euler3d_set3c.jl:1227-1232 (CPU
+ * semantics euler3d_set3c.jl:253-339). */
+int cb_volumerhs(int dim, int N, double *rhs, const double *Q,
+                 const double *vgeo, const double *D, int64_t nelem,
+                 const cb_phys *phys, cb_stream_t stream);
+int cb_volumerhs_f32(int dim, int N, float *rhs, const float *Q,
+                     const float *vgeo, const float *D, int64_t nelem,
+                     const cb_phys *phys, cb_stream_t stream);
+
+/* rhs -= sMJ · Rusanov flux at every face node of every element.
+ * Replaces fluxrhs!(Val(dim), Val(N), d_rhsL::CuArray, d_QL, d_sgeo, d_vgeoL,
+ * elems, d_vmapM, d_vmapP, d_elemtobndy): euler2d_set3c.jl:982-988 /
+ * euler3d_set3c.jl:1234-1240 (CPU semantics euler3d_set3c.jl:342-458). */
+int cb_fluxrhs(int dim, int N, double *rhs, const double *Q,
+               const double *sgeo, const double *vgeo, int64_t nelem,
+               const int64_t *vmapM, const int64_t *vmapP,
+               const int64_t *elemtobndy, const cb_phys *phys,
+               cb_stream_t stream);
+int cb_fluxrhs_f32(int dim, int N, float *rhs, const float *Q,
+                   const float *sgeo, const float *vgeo, int64_t nelem,
+                   const int64_t *vmapM, const int64_t *vmapP,
+                   const int64_t *elemtobndy, const cb_phys *phys,
+                   cb_stream_t stream);
+
+/* rhs += visc·rhs_gradQ[:,:,1,:] (skipped when rhs_gradQ is NULL);
+ * Q += rkb·dt·rhs·MJI; rhs *= rka.
+ * Replaces updatesolution!(Val(dim), Val(N), d_rhsL::CuArray, d_rhs_gradQL,
+ * d_QL, d_vgeoL, elems, rka, rkb, dt, visc): euler3d_set3c.jl:862-872 /
+ * nse2d.jl:806-814 (GPU form euler2d_set3c.jl:990-996). */
+int cb_updatesolution(int dim, int N, double *rhs, const double *rhs_gradQ,
+                      double *Q, const double *vgeo, int64_t nelem, double rka,
+                      double rkb, double dt, double visc, cb_stream_t stream);
+int cb_updatesolution_f32(int dim, int N, float *rhs, const float *rhs_gradQ,
+                          float *Q, const float *vgeo, int64_t nelem,
+                          double rka, double rkb, double dt, double visc,
+                          cb_stream_t stream);
+
+/* LDG Navier–Stokes passes (nse2d.jl:396-778, nse3d.jl:475-970).
+ * volume_grad! zeroes rhs (Np,nstate,dim,nelem) and writes -Dᵀ(MJ ξ·q̂) of the
+ * primitives q̂ = (u,v,[w],ρ,T); flux_grad! adds the central trace term;
+ * update_gradQ! scales by MJI; volume_div!/flux_div! build the divergence of
+ * the viscous stress / heat flux into rhs[:,:,1,:]. */
+int cb_volume_grad(int dim, int N, double *rhs, const double *Q,
+                   const double *vgeo, const double *D, int64_t nelem,
+                   const cb_phys *phys, cb_stream_t stream);
+int cb_flux_grad(int dim, int N, double *rhs, const double *Q,
+                 const double *sgeo, const double *vgeo, int64_t nelem,
+                 const int64_t *vmapM, const int64_t *vmapP,
+                 const int64_t *elemtobndy, const cb_phys *phys,
+                 cb_stream_t stream);
+int cb_update_gradQ(int dim, int N, double *gradQ, const double *rhs,
+                    const double *vgeo, int64_t nelem, cb_stream_t stream);
+int cb_volume_div(int dim, int N, double *rhs, const double *gradQ,
+                  const double *Q, const double *vgeo, const double *D,
+                  int64_t nelem, const cb_phys *phys, cb_stream_t stream);
+int cb_flux_div(int dim, int N, double *rhs, const double *gradQ,
+                const double *Q, const double *sgeo, int64_t nelem,
+                const int64_t *vmapM, const int64_t *vmapP,
+                const int64_t *elemtobndy, const cb_phys *phys,
+                cb_stream_t stream);
+
+/* ---------------------------------------------------------------------- */
+/* Fused, graph-captured LSRK(5,4) driver (drop-in for lowstorageRK).      */
+/* ---------------------------------------------------------------------- */
+
+/* Opaque solver bound to one mesh and one caller-owned state.
+ * Replaces lowstorageRK(Val(dim), Val(N), mesh, vgeo, sgeo, Q, rhs, D, dt,
+ * nsteps, tout, vmapM, vmapP, mpicomm, iplot, visc; ArrType=CuArray):
+ * euler3d_set3c.jl:1361-1523, nse2d.jl:1728-1890.
+ *
+ * precision = 64: Q/rhs are double and vgeo/sgeo/D are used as given.
+ * precision = 32: Q/rhs are float; vgeo/sgeo/D are the FP64 arrays, rounded
+ *                 once into solver-owned FP32 copies.
+ * The solver owns its scratch (a second state buffer for the double-buffered
+ * stage, compact int32 face-neighbour tables built from vmapM/vmapP, the
+ * gradient arrays of the viscous form and the captured CUDA graph). */
+typedef struct cb_solver cb_solver;
+
+int cb_solver_create(cb_solver **out, int dim, int N, int precision,
+                     int64_t nelem, void *Q, void *rhs, const double *vgeo,
+                     const double *sgeo, const int64_t *vmapM,
+                     const int64_t *vmapP, const int64_t *elemtobndy,
+                     const double *D, const cb_phys *phys,
+                     cb_stream_t stream);
+/* Advance Q and the residual carry rhs by nsteps LSRK(5,4) steps of size dt.
+ * Asynchronous; the first call for a given dt captures one step into a CUDA
+ * graph that later calls replay. */
+int cb_lsrk_run(cb_solver *s, int64_t nsteps, double dt);
+/* Compensated (Neumaier) FP64 sums over all nodes of MJ·Q[:,s,:] and
+ * MJ·Q[:,s,:]² for every state field s: out[2*nstate]; synchronises. */
+int cb_solver_sums(cb_solver *s, double *out_host);
+int cb_solver_destroy(cb_solver *s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

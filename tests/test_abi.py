@@ -1,0 +1,60 @@
+"""The C-ABI library loads on a machine without a GPU and exports every
+symbol that include/canary_b200.h declares; argument validation answers
+without touching the device."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+from canary_b200 import _lib
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                      "include", "canary_b200.h")
+
+
+def declared_symbols():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(cb_[A-Za-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_entry_points():
+    syms = declared_symbols()
+    assert "cb_volumerhs" in syms and "cb_lsrk_run" in syms
+    assert set(syms) == set(_lib.EXPORTS)
+
+
+def test_library_exports_every_declared_symbol():
+    L = _lib.lib()
+    for s in declared_symbols():
+        assert hasattr(L, s), s
+
+
+def test_version_and_orders():
+    L = _lib.lib()
+    assert L.cb_version() >= 1
+    assert L.cb_max_order(2) >= 8 and L.cb_max_order(3) >= 10
+    assert L.cb_max_order(4) == 0
+
+
+def test_argument_validation_without_device():
+    L = _lib.lib()
+    phys = _lib.cb_phys(1.4, 1.0, 3.5, 2.5, 0.0, 0.72, -2 / 3, 0.0)
+    dummy = C.c_void_p(16)  # never dereferenced: validation fails first
+    assert L.cb_volumerhs(4, 3, dummy, dummy, dummy, dummy, 1, C.byref(phys), None) == _lib.CB_ERR_ARG
+    assert "dim" in L.cb_last_error().decode()
+    assert L.cb_volumerhs(3, 99, dummy, dummy, dummy, dummy, 1, C.byref(phys), None) == _lib.CB_ERR_UNSUPPORTED
+    assert L.cb_volumerhs(3, 3, None, dummy, dummy, dummy, 1, C.byref(phys), None) == _lib.CB_ERR_ARG
+    assert L.cb_volumerhs(3, 3, dummy, dummy, dummy, dummy, -1, C.byref(phys), None) == _lib.CB_ERR_ARG
+    h = C.c_void_p()
+    assert L.cb_solver_create(C.byref(h), 3, 3, 16, 1, dummy, dummy, dummy, dummy, dummy, dummy,
+                              dummy, dummy, C.byref(phys), None) == _lib.CB_ERR_ARG
+    assert L.cb_lsrk_run(None, 1, 0.1) == _lib.CB_ERR_ARG
+
+
+def test_check_raises():
+    with pytest.raises(_lib.CanaryError):
+        L = _lib.lib()
+        phys = _lib.cb_phys(1.4, 1.0, 3.5, 2.5, 0.0, 0.72, -2 / 3, 0.0)
+        _lib.check(L.cb_volumerhs(5, 3, None, None, None, None, 1, C.byref(phys), None))
