@@ -249,9 +249,8 @@ def main():
     mesh, Q, dt = setup_workload(args.n_side, N, device=dev)
     dm = dg.DeviceMesh.upload(mesh, device=dev)
     real = torch.float64 if args.precision == 64 else torch.float32
-    dQ = dg.to_device(Q, real, dev)
-    drhs = torch.zeros_like(dQ)
-    solver = dg.LSRK(dm, dQ, drhs, args.precision, dg.make_phys(), stream)
+    solver = dg.LSRK.for_state(dm, Q, args.precision, dg.make_phys(), stream)
+    dQ, drhs = solver.Q, solver.rhs
     dof = mesh.nelem * mesh.Np * 5
 
     solver.run(args.warmup, dt)

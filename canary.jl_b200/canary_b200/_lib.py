@@ -23,7 +23,8 @@ EXPORTS = (
     "cb_volumerhs", "cb_volumerhs_f32", "cb_fluxrhs", "cb_fluxrhs_f32",
     "cb_updatesolution", "cb_updatesolution_f32",
     "cb_volume_grad", "cb_flux_grad", "cb_update_gradQ", "cb_volume_div", "cb_flux_div",
-    "cb_solver_create", "cb_lsrk_run", "cb_solver_sums", "cb_solver_destroy",
+    "cb_solver_create", "cb_lsrk_run", "cb_solver_set_offset", "cb_solver_sums",
+    "cb_solver_destroy",
 )
 
 
@@ -74,6 +75,7 @@ def lib() -> C.CDLL:
                                    vp, vp, vp, vp, phys_p, vp]
     L.cb_lsrk_run.argtypes = [vp, i64, dbl]
     L.cb_solver_sums.argtypes = [vp, C.POINTER(C.c_double)]
+    L.cb_solver_set_offset.argtypes = [vp, C.POINTER(C.c_double)]
     L.cb_solver_destroy.argtypes = [vp]
     _lib = L
     return L

@@ -279,6 +279,40 @@ class LSRK:
             _ptr(dmesh.elemtobndy, torch.int64), _ptr(dmesh.D, torch.float64),
             C.byref(self.phys), _stream(stream)))
 
+    @classmethod
+    def for_state(cls, dmesh: DeviceMesh, Q: np.ndarray, precision=64, phys=None, stream=None,
+                  offset=None):
+        """Solver for a host state Q (Np, nstate, nelem).  For precision 32 the
+        device state holds Q - qref with qref = per-field mean of Q (unless
+        `offset` is given), which keeps the FP32 update's rounding relative to
+        the deviation; `state()` returns the full FP64 state."""
+        torch = _torch()
+        Q = np.asarray(Q, dtype=np.float64)
+        ns = Q.shape[1]
+        if offset is None:
+            offset = Q.mean(axis=(0, 2)) if precision == 32 else np.zeros(ns)
+        offset = np.asarray(offset, dtype=np.float64)
+        real = torch.float64 if precision == 64 else torch.float32
+        dev = dmesh.vgeo.device
+        dQ = to_device(Q - offset[None, :, None], real, dev)
+        drhs = torch.zeros_like(dQ)
+        s = cls(dmesh, dQ, drhs, precision, phys, stream)
+        s.set_offset(offset)
+        return s
+
+    def set_offset(self, qref) -> None:
+        ns = nstate(self.dmesh.mesh.dim)
+        arr = (C.c_double * 5)(*([float(v) for v in qref] + [0.0] * (5 - ns)))
+        check(_lib.lib().cb_solver_set_offset(self._h, arr))
+        self.offset = np.array(list(qref)[:ns], dtype=np.float64)
+
+    def state(self) -> np.ndarray:
+        """Full FP64 state (Np, nstate, nelem) on the host."""
+        m = self.dmesh.mesh
+        shape = (m.Np, nstate(m.dim), m.nelem)
+        off = getattr(self, "offset", np.zeros(shape[1]))
+        return from_device(self.Q.double(), shape) + off[None, :, None]
+
     def run(self, nsteps: int, dt: float) -> None:
         check(_lib.lib().cb_lsrk_run(self._h, int(nsteps), float(dt)))
 

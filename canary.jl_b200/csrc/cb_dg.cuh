@@ -39,6 +39,14 @@ struct Lay<2> {
 // vgeo field of metric term d(r-th reference coordinate)/d(x_c): r + DIM*c;
 // MJ = DIM*DIM, MJI = DIM*DIM+1, coordinates from DIM*DIM+2.
 
+// Per-field constants subtracted from the stored state (Q = qref + q').  The
+// FP32 form keeps q' so that each stage's rounding is relative to the
+// deviation instead of the full state; the FP64 form uses qref = 0.
+template <typename T, int NS>
+struct Offs {
+  T v[NS];
+};
+
 template <typename T>
 struct PhysT {
   T gamma, eos, grav, R, cpPr, lambda, visc;

@@ -116,6 +116,12 @@ k_fluxrhs(T *__restrict__ rhs, const T *__restrict__ Q,
     T PP;
     const int64_t bc = elemtobndy[f + NF * e];
     T out[NS];
+    if ((idM - 1) / Np != e || idM < 1 || (bc == 0 && (idP < 1 || eP >= nelem))) {
+      atomicOr(status, ST_MESH);  // vmapP points outside the mesh: skip the face
+#pragma unroll
+      for (int s = 0; s < NS; ++s) FF[(f * NS + s) * FS + el * Nfp + fn] = T(0);
+      continue;
+    }
     if (bc == 0) {
 #pragma unroll
       for (int s = 0; s < NS; ++s) qP[s] = Q[vP + Np * (s + NS * eP)];
@@ -186,7 +192,8 @@ __global__ void __launch_bounds__(Cfg<DIM, Nq>::THREADS)
 k_stage(const T *__restrict__ Qin, T *__restrict__ Qout, T *__restrict__ rhs,
         const T *__restrict__ vgeo, const T *__restrict__ sgeo,
         const int32_t *__restrict__ nbr, const T *__restrict__ D,
-        int64_t nelem, PhysT<T> p, T rka, T rkbdt, unsigned *status) {
+        int64_t nelem, PhysT<T> p, Offs<T, Lay<DIM>::NS> qref, T rka, T rkbdt,
+        unsigned *status) {
   using C = Cfg<DIM, Nq>;
   constexpr int NS = Lay<DIM>::NS, NVG = Lay<DIM>::NVG, NSG = Lay<DIM>::NSG;
   constexpr int Np = C::Np, Nfp = C::Nfp, NF = C::NFACE, SP = C::SLOTS;
@@ -209,8 +216,9 @@ k_stage(const T *__restrict__ Qin, T *__restrict__ Qout, T *__restrict__ rhs,
       T q[NS];
 #pragma unroll
       for (int s = 0; s < NS; ++s) {
-        q[s] = Qin[n + Np * (s + NS * e)];
-        sQ[s * SP + slot] = q[s];
+        const T d = Qin[n + Np * (s + NS * e)];
+        sQ[s * SP + slot] = d;
+        q[s] = d + qref.v[s];
         R[u][s] = rhs[n + Np * (s + NS * e)];
       }
       pointwise_euler<DIM, Nq, C::EPB, T>(q, vgeo + (int64_t)Np * NVG * e, n, el, sF, p, R[u]);
@@ -242,7 +250,7 @@ k_stage(const T *__restrict__ Qin, T *__restrict__ Qout, T *__restrict__ rhs,
     const T sMJ = sg[DIM];
     T qM[NS], qP[NS];
 #pragma unroll
-    for (int s = 0; s < NS; ++s) qM[s] = sQ[s * SP + el * Np + vM];
+    for (int s = 0; s < NS; ++s) qM[s] = sQ[s * SP + el * Np + vM] + qref.v[s];
     const T gM = p.grav != T(0) ? vgeo[vM + Np * (GC + NVG * e)] : T(0);
     const T PM = pressure<DIM, T>(qM, gM, p);
     const int32_t nb = nbr[f + NF * e];
@@ -251,7 +259,7 @@ k_stage(const T *__restrict__ Qin, T *__restrict__ Qout, T *__restrict__ rhs,
       const int64_t e2 = nb >> 3;
       const int vP = face_node<DIM, Nq>(nb & 7, fn);
 #pragma unroll
-      for (int s = 0; s < NS; ++s) qP[s] = Qin[vP + Np * (s + NS * e2)];
+      for (int s = 0; s < NS; ++s) qP[s] = Qin[vP + Np * (s + NS * e2)] + qref.v[s];
       const T gP = p.grav != T(0) ? vgeo[vP + Np * (GC + NVG * e2)] : T(0);
       PP = pressure<DIM, T>(qP, gP, p);
     } else {
@@ -436,6 +444,11 @@ k_flux_grad(T *__restrict__ rhs, const T *__restrict__ Q,
     const T gM = p.grav != T(0) ? vgeo[vM + Np * (GC + NVG * e)] : T(0);
     primitives<DIM, T>(qM, gM, p, pM);
     const int64_t bc = elemtobndy[f + NF * e];
+    if ((idM - 1) / Np != e || idM < 1 || (bc == 0 && (idP < 1 || eP >= nelem))) {
+      atomicOr(status, ST_MESH);
+      for (int s = 0; s < NS * DIM; ++s) FF[(f * NS * DIM + s) * FS + el * Nfp + fn] = T(0);
+      continue;
+    }
     if (bc == 0) {
       T qP[NS];
 #pragma unroll
@@ -620,6 +633,11 @@ k_flux_div(T *__restrict__ rhs, const T *__restrict__ gradQ,
 #pragma unroll
     for (int c = 0; c < DIM; ++c) vM_[c] = Q[vM + Np * (c + NS * e)] / rhoM;
     const int64_t bc = elemtobndy[f + NF * e];
+    if ((idM - 1) / Np != e || idM < 1 || (bc == 0 && (idP < 1 || eP >= nelem))) {
+      atomicOr(status, ST_MESH);
+      for (int s = 0; s < NS; ++s) FF[(f * NS + s) * FS + el * Nfp + fn] = T(0);
+      continue;
+    }
     if (bc == 0) {
 #pragma unroll
       for (int s = 0; s < NS; ++s)
@@ -697,7 +715,8 @@ __device__ __forceinline__ void neu_merge(double &sum, double &comp, double s2, 
 }
 template <int DIM, typename T>
 __global__ void __launch_bounds__(256) k_cons_sums(const T *__restrict__ Q, const T *__restrict__ vgeo,
-                                                   int64_t nelem, int Np, double *__restrict__ part) {
+                                                   int64_t nelem, int Np, Offs<double, Lay<DIM>::NS> qref,
+                                                   double *__restrict__ part) {
   constexpr int NS = Lay<DIM>::NS, NVG = Lay<DIM>::NVG, MJ = DIM * DIM;
   double acc[4 * NS];
   for (int s = 0; s < 4 * NS; ++s) acc[s] = 0.0;
@@ -707,7 +726,7 @@ __global__ void __launch_bounds__(256) k_cons_sums(const T *__restrict__ Q, cons
     const int64_t n = q % Np, e = q / Np;
     const double mj = (double)vgeo[n + Np * (MJ + (int64_t)NVG * e)];
     for (int s = 0; s < NS; ++s) {
-      const double v = (double)Q[n + Np * (s + (int64_t)NS * e)];
+      const double v = (double)Q[n + Np * (s + (int64_t)NS * e)] + qref.v[s];
       neu_add(acc[4 * s + 0], acc[4 * s + 1], mj * v);
       neu_add(acc[4 * s + 2], acc[4 * s + 3], mj * (v * v));
     }
@@ -733,6 +752,10 @@ __global__ void __launch_bounds__(256) k_cons_sums(const T *__restrict__ Q, cons
 
 // Rounds an FP64 array to FP32.
 __global__ void k_round_f32(float *__restrict__ dst, const double *__restrict__ src, int64_t n);
+
+}  // namespace cb
+#include "cb_pipe.cuh"
+namespace cb {
 
 // ---------------------------------------------------------------- launchers
 template <int DIM, int Nq, typename T>
@@ -771,13 +794,29 @@ struct Launch {
   }
   static cudaError_t stage(const T *Qin, T *Qout, T *rhs, const T *vgeo, const T *sgeo,
                            const int32_t *nbr, const T *D, int64_t nelem, const PhysT<T> &p,
-                           T rka, T rkbdt, unsigned *status, cudaStream_t st) {
-    size_t sm = smem_stage();
-    cudaError_t err = prep(k_stage<DIM, Nq, T>, sm);
-    if (err != cudaSuccess) return err;
-    k_stage<DIM, Nq, T><<<grid(nelem), C::THREADS, sm, st>>>(Qin, Qout, rhs, vgeo, sgeo, nbr, D,
-                                                              nelem, p, rka, rkbdt, status);
-    return cudaGetLastError();
+                           const Offs<T, NS> &qref, T rka, T rkbdt, unsigned *status,
+                           cudaStream_t st) {
+    constexpr bool pipe_ok = Pipe<DIM, Nq, T>::OK;
+    const bool aligned = ((reinterpret_cast<uintptr_t>(Qin) | reinterpret_cast<uintptr_t>(vgeo)) & 15) == 0;
+    if (pipe_ok && aligned) {
+      using PP = Pipe<DIM, Nq, T>;
+      size_t sm = PP::smem();
+      cudaError_t err = prep(k_stage_pipe<DIM, Nq, T>, sm);
+      if (err != cudaSuccess) return err;
+      const int64_t groups = (nelem + C::EPB - 1) / C::EPB;
+      int g = num_sms();
+      if ((int64_t)g > groups) g = (int)groups;
+      k_stage_pipe<DIM, Nq, T><<<g, C::THREADS, sm, st>>>(Qin, Qout, rhs, vgeo, sgeo, nbr, D, nelem,
+                                                          p, qref, rka, rkbdt, status);
+      return cudaGetLastError();
+    } else {
+      size_t sm = smem_stage();
+      cudaError_t err = prep(k_stage<DIM, Nq, T>, sm);
+      if (err != cudaSuccess) return err;
+      k_stage<DIM, Nq, T><<<grid(nelem), C::THREADS, sm, st>>>(Qin, Qout, rhs, vgeo, sgeo, nbr, D,
+                                                                nelem, p, qref, rka, rkbdt, status);
+      return cudaGetLastError();
+    }
   }
   static cudaError_t build_nbr(int32_t *nbr, const int64_t *vmapM, const int64_t *vmapP,
                                const int64_t *bnd, int64_t nelem, unsigned *status,

@@ -16,7 +16,7 @@ struct Ops {
   cudaError_t (*fluxrhs)(T *, const T *, const T *, const T *, int64_t, const int64_t *,
                          const int64_t *, const int64_t *, const PhysT<T> &, unsigned *, cudaStream_t);
   cudaError_t (*stage)(const T *, T *, T *, const T *, const T *, const int32_t *, const T *, int64_t,
-                       const PhysT<T> &, T, T, unsigned *, cudaStream_t);
+                       const PhysT<T> &, const Offs<T, 5> &, T, T, unsigned *, cudaStream_t);
   cudaError_t (*build_nbr)(int32_t *, const int64_t *, const int64_t *, const int64_t *, int64_t,
                            unsigned *, cudaStream_t);
   cudaError_t (*volume_grad)(T *, const T *, const T *, const T *, int64_t, const PhysT<T> &, cudaStream_t);
@@ -29,7 +29,8 @@ struct Ops {
   // order-independent element-wise kernels
   cudaError_t (*update)(T *, const T *, T *, const T *, int64_t, int, T, T, T, T, cudaStream_t);
   cudaError_t (*update_gradQ)(T *, const T *, const T *, int64_t, int, cudaStream_t);
-  cudaError_t (*cons_sums)(const T *, const T *, int64_t, int, double *, int, cudaStream_t);
+  cudaError_t (*cons_sums)(const T *, const T *, int64_t, int, const Offs<double, 5> &, double *, int,
+                           cudaStream_t);
 };
 
 // Defined in cb_inst_<dim>d_<prec>.cu; nullptr when N is outside 1..MAXN.

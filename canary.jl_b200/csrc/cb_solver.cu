@@ -43,6 +43,7 @@ struct cb_solver {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   double graph_dt = NAN;
+  double qref[5] = {0, 0, 0, 0, 0};  // stored state = Q - qref
 };
 
 namespace {
@@ -80,8 +81,10 @@ cudaError_t enqueue_step(cb_solver *s, double dt, bool from_user) {
     return e;
   }
   T *a = (T *)(from_user ? s->Q : s->Qalt), *b = (T *)(from_user ? s->Qalt : s->Q);
+  Offs<T, 5> q5;
+  for (int k = 0; k < 5; ++k) q5.v[k] = T(s->qref[k]);
   for (int st = 0; st < 5 && e == cudaSuccess; ++st) {
-    e = o->stage(a, b, (T *)s->rhs, vg, sg, s->nbr, D, s->nelem, p, T(RKA[(st + 1) % 5]),
+    e = o->stage(a, b, (T *)s->rhs, vg, sg, s->nbr, D, s->nelem, p, q5, T(RKA[(st + 1) % 5]),
                  T(RKB[st] * dt), s->status, s->stream);
     T *t = a;
     a = b;
@@ -253,9 +256,11 @@ int cb_solver_sums(cb_solver *s, double *out_host) {
   if (!s || !out_host) return solver_fail(CB_ERR_ARG, "null argument");
   const int ns = s->dim == 2 ? 4 : 5, Nq = s->N + 1;
   const int Np = s->dim == 2 ? Nq * Nq : Nq * Nq * Nq;
+  Offs<double, 5> q5;
+  for (int k = 0; k < 5; ++k) q5.v[k] = s->qref[k];
   cudaError_t e = s->prec == 64
-                      ? ops<double>(s)->cons_sums((const double *)s->Q, (const double *)s->vgeo, s->nelem, Np, s->part, s->part_blocks, s->stream)
-                      : ops<float>(s)->cons_sums((const float *)s->Q, (const float *)s->vgeo, s->nelem, Np, s->part, s->part_blocks, s->stream);
+                      ? ops<double>(s)->cons_sums((const double *)s->Q, (const double *)s->vgeo, s->nelem, Np, q5, s->part, s->part_blocks, s->stream)
+                      : ops<float>(s)->cons_sums((const float *)s->Q, (const float *)s->vgeo, s->nelem, Np, q5, s->part, s->part_blocks, s->stream);
   if (e != cudaSuccess) return solver_fail(CB_ERR_CUDA, "sums launch: %s", cudaGetErrorString(e));
   std::string buf(sizeof(double) * 4 * ns * s->part_blocks, '\0');
   double *h = (double *)&buf[0];
@@ -279,6 +284,18 @@ int cb_solver_sums(cb_solver *s, double *out_host) {
   }
   if (st & ST_NONFINITE) return solver_fail(CB_ERR_NONFINITE, "the state became non-finite");
   if (st & ST_BC) return solver_fail(CB_ERR_BC, "invalid boundary condition code");
+  return CB_OK;
+}
+
+int cb_solver_set_offset(cb_solver *s, const double *qref) {
+  if (!s || !qref) return solver_fail(CB_ERR_ARG, "null argument");
+  if (s->phys.visc > 0) {
+    for (int k = 0; k < (s->dim == 2 ? 4 : 5); ++k)
+      if (qref[k] != 0.0) return solver_fail(CB_ERR_UNSUPPORTED, "state offsets are supported by the inviscid form only");
+    return CB_OK;
+  }
+  for (int k = 0; k < (s->dim == 2 ? 4 : 5); ++k) s->qref[k] = qref[k];
+  drop_graph(s);
   return CB_OK;
 }
 

@@ -170,6 +170,13 @@ int cb_solver_create(cb_solver **out, int dim, int N, int precision,
  * Asynchronous; the first call for a given dt captures one step into a CUDA
  * graph that later calls replay. */
 int cb_lsrk_run(cb_solver *s, int64_t nsteps, double dt);
+/* Per-field constants qref[nstate] (host array) for the stored state: the
+ * state array then holds Q - qref and the kernels add qref back when they form
+ * fluxes.  Used by the FP32 form so that the per-stage rounding of the update
+ * is relative to the deviation from a reference state (e.g. the free stream)
+ * rather than to the full state; FP64 solvers leave it at zero.  Inviscid
+ * form only.  The conservation sums below are reported for the full Q. */
+int cb_solver_set_offset(cb_solver *s, const double *qref);
 /* Compensated (Neumaier) FP64 sums over all nodes of MJ·Q[:,s,:] and
  * MJ·Q[:,s,:]² for every state field s: out[2*nstate]; synchronises. */
 int cb_solver_sums(cb_solver *s, double *out_host);

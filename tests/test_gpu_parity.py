@@ -152,15 +152,18 @@ def test_fused_lsrk_vortex_500_steps():
     s.close()
 
 
-@pytest.mark.parametrize("nsteps", [1, 4, 7])
-def test_fused_lsrk_3d_warped(nsteps):
-    N = 7
-    m = make_mesh(3, N, n=4, L=2 * math.pi)
+@pytest.mark.parametrize("N,n,nsteps", [(7, 4, 1), (7, 4, 7), (7, 8, 4), (4, 6, 3), (3, 6, 2), (10, 2, 2)])
+def test_fused_lsrk_3d_warped(N, n, nsteps):
+    """Fused driver on warped periodic cubes; n=8 at N=7 gives more elements
+    than SMs so every block runs several pipelined iterations; N=4 and N=3
+    stage through per-thread async copies (slab sizes not 16-byte multiples)
+    and N=10 uses the non-pipelined stage kernel."""
+    m = make_mesh(3, N, n=n, L=2 * math.pi)
     x, y, z = m.coords()
     U, V, W, rho, E = ic.fourier_state(x, y, z, seed=0)
     Q = np.zeros((m.Np, 5, m.nelem), order="F")
     Q[:, 0], Q[:, 1], Q[:, 2], Q[:, 3], Q[:, 4] = U, V, W, rho, E
-    dt = ic.fourier_dt(Q, N, h=2 * math.pi / 4)
+    dt = ic.fourier_dt(Q, N, h=2 * math.pi / n)
     ref, rref = Q.copy(order="F"), np.zeros_like(Q, order="F")
     O.lowstorageRK(3, N, m.vgeo, m.sgeo, ref, rref, m.D, dt, nsteps, m.vmapM, m.vmapP,
                    m.elemtobndy, oracle_phys(dg.WORKLOAD_PHYS), NT)
@@ -172,19 +175,59 @@ def test_fused_lsrk_3d_warped(nsteps):
     s.close()
 
 
+@pytest.mark.parametrize("n_side,N", [(40, 4), (24, 3), (16, 7)])
+def test_fused_lsrk_2d_many_blocks(n_side, N):
+    """2-D vortex on finer meshes: more element groups than SMs, so the
+    pipelined stage kernel iterates."""
+    m = dg.build_mesh(2, N, (np.linspace(0, 10, n_side + 1),) * 2, (True, True))
+    x, y = m.coords()
+    U, V, rho, E = ic.isentropic_vortex(x, y)
+    Q = np.zeros((m.Np, 4, m.nelem), order="F")
+    Q[:, 0], Q[:, 1], Q[:, 2], Q[:, 3] = U, V, rho, E
+    ref, rref = Q.copy(order="F"), np.zeros_like(Q, order="F")
+    O.lowstorageRK(2, N, m.vgeo, m.sgeo, ref, rref, m.D, 0.001, 60, m.vmapM, m.vmapP,
+                   m.elemtobndy, oracle_phys(dg.WORKLOAD_PHYS), NT)
+    s = dg.LSRK(dg.DeviceMesh.upload(m), dev(Q), dev(np.zeros_like(Q)), 64)
+    s.run(60, 0.001)
+    assert relerr(dg.from_device(s.Q, Q.shape), ref) < 1e-12
+    s.close()
+
+
 def test_fp32_precision_form_vortex():
     m, Q = vortex_setup()
     ref, rref = Q.copy(order="F"), np.zeros_like(Q, order="F")
     O.lowstorageRK(2, 4, m.vgeo, m.sgeo, ref, rref, m.D, 0.002, 500, m.vmapM, m.vmapP,
                    m.elemtobndy, oracle_phys(dg.WORKLOAD_PHYS), NT)
-    import torch
     dm = dg.DeviceMesh.upload(m)
-    dQ = dev(Q, torch.float32)
-    drhs = torch.zeros_like(dQ)
-    s = dg.LSRK(dm, dQ, drhs, 32)
+    s = dg.LSRK.for_state(dm, Q, 32)
     s.run(500, 0.002)
-    out = dg.from_device(dQ.double(), Q.shape)
-    assert relerr(out, ref) < 1e-5
+    out = s.state()
+    errs = [np.linalg.norm(out[:, q] - ref[:, q]) / np.linalg.norm(ref[:, q]) for q in range(4)]
+    print("fp32 rel L2 per field (U, V, rho, E):", errs)
+    assert max(errs) < 1e-5
+    sums = s.sums()
+    mj = m.vgeo[:, 4, :]
+    assert np.allclose(sums[0], [(mj * out[:, q]).sum() for q in range(4)], rtol=1e-6)
+    s.close()
+
+
+def test_fp32_precision_form_3d_fourier():
+    N = 7
+    m = make_mesh(3, N, n=4, L=2 * math.pi)
+    x, y, z = m.coords()
+    U, V, W, rho, E = ic.fourier_state(x, y, z, seed=0)
+    Q = np.zeros((m.Np, 5, m.nelem), order="F")
+    Q[:, 0], Q[:, 1], Q[:, 2], Q[:, 3], Q[:, 4] = U, V, W, rho, E
+    dt = ic.fourier_dt(Q, N, h=2 * math.pi / 4)
+    ref, rref = Q.copy(order="F"), np.zeros_like(Q, order="F")
+    O.lowstorageRK(3, N, m.vgeo, m.sgeo, ref, rref, m.D, dt, 40, m.vmapM, m.vmapP,
+                   m.elemtobndy, oracle_phys(dg.WORKLOAD_PHYS), NT)
+    s = dg.LSRK.for_state(dg.DeviceMesh.upload(m), Q, 32)
+    s.run(40, dt)
+    out = s.state()
+    errs = [np.linalg.norm(out[:, q] - ref[:, q]) / np.linalg.norm(ref[:, q]) for q in range(5)]
+    print("fp32 3-D rel L2 per field:", errs)
+    assert max(errs) < 1e-5
     s.close()
 
 
@@ -279,7 +322,7 @@ def test_nonconforming_vmap_is_rejected():
 
 def test_zero_elements_is_a_noop():
     import torch
-    t = torch.zeros(8, dtype=torch.float64, device="cuda")
+    t = torch.zeros(64, dtype=torch.float64, device="cuda")
     dg.volumerhs(3, 3, t, t, t, t, 0)
     dg.updatesolution(3, 3, t, None, t, t, 0, 0.1, 0.2, 0.3)
     assert torch.all(t == 0)
