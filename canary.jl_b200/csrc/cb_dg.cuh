@@ -105,6 +105,85 @@ __device__ __forceinline__ void euler_flux(const T *q, T P, T (*f)[DIM]) {
   }
 }
 
+// Variants for the fused stage: 1/ρ is formed once per state and reused by the
+// pressure, the fluxes and the wave speed (one FP64 division per state
+// instead of two; rounding differs from the reference's `/(2ρ)` by <= 1 ulp).
+template <int DIM, typename T>
+__device__ __forceinline__ T pressure_ri(const T *q, T ri, T gc, const PhysT<T> &p) {
+  constexpr int IR = Lay<DIM>::IR, IE = Lay<DIM>::IE;
+  T ke = q[0] * q[0] + q[1] * q[1];
+  if (DIM == 3) ke = ke + q[2] * q[2];
+  return p.eos * ((q[IE] - T(0.5) * ke * ri) - q[IR] * p.grav * gc);
+}
+template <int DIM, typename T>
+__device__ __forceinline__ void euler_flux_ri(const T *q, T ri, T P, T (*f)[DIM]) {
+  constexpr int IR = Lay<DIM>::IR, IE = Lay<DIM>::IE;
+#pragma unroll
+  for (int a = 0; a < DIM; ++a) {
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      T v = ri * q[a] * q[c];
+      if (a == c) v = v + P;
+      f[a][c] = v;
+    }
+    f[IR][a] = q[a];
+    f[IE][a] = ri * q[a] * (q[IE] + P);
+  }
+}
+template <int DIM, typename T>
+__device__ __forceinline__ void rusanov_ri(const T *qM, T rMi, T PM, const T *qP, T rPi, T PP,
+                                           const T *nrm, const PhysT<T> &p, T *out) {
+  constexpr int NS = Lay<DIM>::NS;
+  T fM[NS][DIM], fP[NS][DIM];
+  euler_flux_ri<DIM, T>(qM, rMi, PM, fM);
+  euler_flux_ri<DIM, T>(qP, rPi, PP, fP);
+  T unM = nrm[0] * qM[0] + nrm[1] * qM[1];
+  T unP = nrm[0] * qP[0] + nrm[1] * qP[1];
+  if (DIM == 3) {
+    unM = unM + nrm[2] * qM[2];
+    unP = unP + nrm[2] * qP[2];
+  }
+  const T lM = rMi * fabs(unM) + sqrt(rMi * p.gamma * PM);
+  const T lP = rPi * fabs(unP) + sqrt(rPi * p.gamma * PP);
+  T lam = lM > lP ? lM : lP;
+  if (lM != lM || lP != lP) lam = lM + lP;
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    T a = nrm[0] * (fM[s][0] + fP[s][0]) + nrm[1] * (fM[s][1] + fP[s][1]);
+    if (DIM == 3) a = a + nrm[2] * (fM[s][2] + fP[s][2]);
+    out[s] = (a - lam * (qP[s] - qM[s])) * T(0.5);
+  }
+}
+
+// Normal Euler flux n·F of one state (5 values) given 1/ρ and P: the
+// fused stage uses it instead of forming both 3x5 flux tensors and dotting
+// them with n (same mathematics, about a third of the operations).
+template <int DIM, typename T>
+__device__ __forceinline__ void normal_flux(const T *q, T ri, T P, const T *nrm, T &un, T *fn) {
+  constexpr int IR = Lay<DIM>::IR, IE = Lay<DIM>::IE;
+  un = nrm[0] * q[0] + nrm[1] * q[1];
+  if (DIM == 3) un = un + nrm[2] * q[2];
+  const T riun = ri * un;
+#pragma unroll
+  for (int a = 0; a < DIM; ++a) fn[a] = riun * q[a] + P * nrm[a];
+  fn[IR] = un;
+  fn[IE] = riun * (q[IE] + P);
+}
+template <int DIM, typename T>
+__device__ __forceinline__ void rusanov_n(const T *qM, T rMi, T PM, const T *qP, T rPi, T PP,
+                                          const T *nrm, const PhysT<T> &p, T *out) {
+  constexpr int NS = Lay<DIM>::NS;
+  T fM[NS], fP[NS], unM, unP;
+  normal_flux<DIM, T>(qM, rMi, PM, nrm, unM, fM);
+  normal_flux<DIM, T>(qP, rPi, PP, nrm, unP, fP);
+  const T lM = rMi * fabs(unM) + sqrt(rMi * p.gamma * PM);
+  const T lP = rPi * fabs(unP) + sqrt(rPi * p.gamma * PP);
+  T lam = lM > lP ? lM : lP;
+  if (lM != lM || lP != lP) lam = lM + lP;
+#pragma unroll
+  for (int s = 0; s < NS; ++s) out[s] = ((fM[s] + fP[s]) - lam * (qP[s] - qM[s])) * T(0.5);
+}
+
 // Rusanov numerical flux (euler3d_set3c.jl:394-446): out[s] = n·(F⁻+F⁺)/2 - λ(q⁺-q⁻)/2
 template <int DIM, typename T>
 __device__ __forceinline__ void rusanov(const T *qM, T PM, const T *qP, T PP,

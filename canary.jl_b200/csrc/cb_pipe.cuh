@@ -84,25 +84,93 @@ inline int num_sms() {
 constexpr uint32_t WAIT_LIMIT = 1u << 22;
 constexpr size_t SMEM_LIMIT = 227 * 1024;
 
+// Row stride (in elements) of the contraction buffers: >= Nq, a multiple of
+// the 16-byte vector width, and an odd number of 16-byte chunks so that the
+// rows read by the 8-32 lanes of a warp fall into distinct shared-memory banks.
+template <typename T>
+__host__ __device__ constexpr int row_stride(int nq) {
+  int vw = 16 / (int)sizeof(T), rs = ((nq + vw - 1) / vw) * vw;
+  return ((rs / vw) % 2 == 1) ? rs : rs + vw;
+}
+
 // Shared-memory plan of the pipelined stage for one (dim, Nq, T).
 template <int DIM, int Nq, typename T>
 struct Pipe {
   using C = Cfg<DIM, Nq>;
   static constexpr int NS = Lay<DIM>::NS;
   static constexpr int NG = DIM * DIM + 2;  // staged vgeo fields: metric, MJ, MJI
+  static constexpr int VW = 16 / (int)sizeof(T);   // elements per 16-byte vector
+  static constexpr int MV = ((Nq + VW - 1) / VW) * VW;  // contraction length, padded
+  static constexpr int RS = row_stride<T>(Nq);
+  static constexpr int NR = ipow(Nq, DIM - 1);     // rows per element and field
   static constexpr size_t QB = sizeof(T) * (size_t)C::Np * NS;   // bytes per element
   static constexpr size_t GB = sizeof(T) * (size_t)C::Np * NG;
   static constexpr bool BULK =
       QB % 16 == 0 && GB % 16 == 0 && (sizeof(T) * (size_t)C::Np * Lay<DIM>::NVG) % 16 == 0;
   static constexpr size_t pad16(size_t b) { return (b + 15) & ~size_t(15); }
-  static constexpr size_t OFF_D = 16;
-  static constexpr size_t OFF_ST = OFF_D + pad16(sizeof(T) * Nq * Nq);
+  static constexpr size_t OFF_D = 16;  // D^T rows, padded like the flux rows
+  static constexpr size_t OFF_ST = OFF_D + pad16(sizeof(T) * Nq * RS);
   static constexpr size_t STAGE = C::EPB * (QB + GB);
   static constexpr size_t OFF_F = OFF_ST + 2 * pad16(STAGE);
-  static constexpr size_t FLUX = sizeof(T) * (size_t)DIM * NS * C::SLOTS;
-  static constexpr size_t smem() { return OFF_F + FLUX; }
-  static constexpr bool OK = smem() <= SMEM_LIMIT && C::NFACE * C::Nfp <= DIM * C::Np;
+  static constexpr size_t FDIR = (size_t)NS * C::EPB * NR * RS;  // elements per direction
+  static constexpr size_t FLUX = sizeof(T) * DIM * FDIR;
+  static constexpr size_t FFB = sizeof(T) * (size_t)C::NFACE * NS * C::EPB * C::Nfp;
+  // face fluxes have their own buffer: they are produced in the same phase
+  // as the volume fluxes
+  static constexpr size_t OFF_FF = OFF_F + pad16(FLUX);
+  static constexpr size_t smem() { return OFF_FF + FFB; }
+  static constexpr bool OK = smem() <= SMEM_LIMIT;
 };
+
+template <typename T>
+struct Vec16;
+template <>
+struct Vec16<double> {
+  using type = double2;
+};
+template <>
+struct Vec16<float> {
+  using type = float4;
+};
+
+// Load MV consecutive elements (16-byte aligned) into registers.
+template <typename T, int MV>
+__device__ __forceinline__ void load_row(const T *src, T *dst) {
+  using V = typename Vec16<T>::type;
+  constexpr int VW = 16 / (int)sizeof(T);
+#pragma unroll
+  for (int q = 0; q < MV / VW; ++q) {
+    const V v = reinterpret_cast<const V *>(src)[q];
+    const T *pv = reinterpret_cast<const T *>(&v);
+#pragma unroll
+    for (int t = 0; t < VW; ++t) dst[q * VW + t] = pv[t];
+  }
+}
+
+// Tensor-product contraction of one node from direction-major flux rows:
+// R[s] += Σ_m D[m,i] Fξ[m;j,k] (then η, then ζ), each sum in m order.
+template <int DIM, int Nq, typename T>
+__device__ __forceinline__ void contract_rows(const T *flux, const T *DT, int el, int n, T *R) {
+  using PP = Pipe<DIM, Nq, T>;
+  constexpr int NS = Lay<DIM>::NS, MV = PP::MV, RS = PP::RS, NR = PP::NR, EPB = Cfg<DIM, Nq>::EPB;
+  const int i = n % Nq, j = (n / Nq) % Nq, k = DIM == 3 ? n / (Nq * Nq) : 0;
+#pragma unroll
+  for (int r = 0; r < DIM; ++r) {
+    const int idx = r == 0 ? i : (r == 1 ? j : k);
+    const int row = DIM == 2 ? (r == 0 ? j : i) : (r == 0 ? j + Nq * k : (r == 1 ? i + Nq * k : i + Nq * j));
+    T d[MV];
+    load_row<T, MV>(DT + idx * RS, d);
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      T f[MV];
+      load_row<T, MV>(flux + r * PP::FDIR + ((size_t)(s * EPB + el) * NR + row) * RS, f);
+      T acc = R[s];
+#pragma unroll
+      for (int m = 0; m < MV; ++m) acc += d[m] * f[m];
+      R[s] = acc;
+    }
+  }
+}
 
 template <int DIM, int Nq, typename T>
 __global__ void __launch_bounds__(Cfg<DIM, Nq>::THREADS, 1)
@@ -112,41 +180,40 @@ k_stage_pipe(const T *__restrict__ Qin, T *__restrict__ Qout, T *__restrict__ rh
              PhysT<T> p, Offs<T, Lay<DIM>::NS> qref, T rka, T rkbdt, unsigned *status) {
   using C = Cfg<DIM, Nq>;
   using PP = Pipe<DIM, Nq, T>;
-  constexpr int NS = Lay<DIM>::NS, NVG = Lay<DIM>::NVG, NSG = Lay<DIM>::NSG;
+  constexpr int NS = Lay<DIM>::NS, NVG = Lay<DIM>::NVG, NSG = Lay<DIM>::NSG, IR = Lay<DIM>::IR;
   constexpr int Np = C::Np, Nfp = C::Nfp, NF = C::NFACE, EPB = C::EPB, SP = C::SLOTS;
   constexpr int NG = PP::NG, MJI = DIM * DIM + 1, GC = DIM * DIM + 2 + DIM - 1;
   constexpr int FS = EPB * Nfp;
-  extern __shared__ __align__(128) unsigned char smem_raw[];
+  constexpr int RS = PP::RS, NR = PP::NR;
+  constexpr size_t STRIDE = PP::pad16(PP::STAGE) / sizeof(T);  // elements between the two stages
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
-  T *Ds = reinterpret_cast<T *>(smem_raw + PP::OFF_D);
-  T *stage[2] = {reinterpret_cast<T *>(smem_raw + PP::OFF_ST),
-                 reinterpret_cast<T *>(smem_raw + PP::OFF_ST + PP::pad16(PP::STAGE))};
+  T *DT = reinterpret_cast<T *>(smem_raw + PP::OFF_D);
+  T *stage0 = reinterpret_cast<T *>(smem_raw + PP::OFF_ST);
   T *sF = reinterpret_cast<T *>(smem_raw + PP::OFF_F);
-  T *FF = sF;  // face fluxes reuse the volume-flux buffer
+  T *FF = reinterpret_cast<T *>(smem_raw + PP::OFF_FF);
   const int tid = threadIdx.x;
   const int64_t ngroups = (nelem + EPB - 1) / EPB;
 
-  // stage layout: [EPB][NS][Np] state, then [EPB][NG][Np] geometry
-  auto sQ = [&](int b) { return stage[b]; };
-  auto sG = [&](int b) { return stage[b] + EPB * Np * NS; };
-
+  // stage b layout: [EPB][NS][Np] state, then [EPB][NG][Np] geometry
   auto issue = [&](int64_t g, int b) {
     const int64_t e0 = g * EPB;
     const int nv = (int)((nelem - e0) < EPB ? (nelem - e0) : EPB);
+    T *dq = stage0 + b * STRIDE, *dg = dq + EPB * Np * NS;
     if constexpr (PP::BULK) {
       if (tid == 0) {
         fence_proxy_async();
         mbar_expect_tx(&bars[b], (uint32_t)(nv * (PP::QB + PP::GB)));
-        bulk_g2s(sQ(b), Qin + e0 * Np * NS, (uint32_t)(nv * PP::QB), &bars[b]);
+        bulk_g2s(dq, Qin + e0 * Np * NS, (uint32_t)(nv * PP::QB), &bars[b]);
         for (int el = 0; el < nv; ++el)
-          bulk_g2s(sG(b) + el * Np * NG, vgeo + (e0 + el) * Np * NVG, (uint32_t)PP::GB, &bars[b]);
+          bulk_g2s(dg + el * Np * NG, vgeo + (e0 + el) * Np * NVG, (uint32_t)PP::GB, &bars[b]);
       }
     } else {
       const T *srcQ = Qin + e0 * Np * NS;
-      for (int t = tid; t < nv * Np * NS; t += C::THREADS) cp_async<sizeof(T)>(sQ(b) + t, srcQ + t);
+      for (int t = tid; t < nv * Np * NS; t += C::THREADS) cp_async<sizeof(T)>(dq + t, srcQ + t);
       for (int t = tid; t < nv * Np * NG; t += C::THREADS) {
         const int el = t / (Np * NG), r = t % (Np * NG);
-        cp_async<sizeof(T)>(sG(b) + t, vgeo + (e0 + el) * Np * NVG + r);
+        cp_async<sizeof(T)>(dg + t, vgeo + (e0 + el) * Np * NVG + r);
       }
       cp_async_commit();
     }
@@ -157,11 +224,33 @@ k_stage_pipe(const T *__restrict__ Qin, T *__restrict__ Qout, T *__restrict__ rh
     mbar_init(&bars[1], 1);
     fence_mbar_init();
   }
-  load_D(Ds, D, Nq * Nq);
+  // D^T rows (DT[i][m] = D[m, i]) and the padded flux columns start at zero
+  for (int t = tid; t < Nq * RS; t += C::THREADS) {
+    const int i = t / RS, m = t % RS;
+    DT[t] = m < Nq ? D[m + Nq * i] : T(0);
+  }
+  if constexpr (PP::MV > Nq)
+    for (size_t t = tid; t < (size_t)DIM * PP::FDIR; t += C::THREADS)
+      if ((int)(t % RS) >= Nq) sF[t] = T(0);
   __syncthreads();
   if ((int64_t)blockIdx.x < ngroups) issue(blockIdx.x, 0);
 
-  bool bad = false;
+  // neighbour codes of this thread's face slots, loaded one group ahead so
+  // that the dependent neighbour-trace loads can start at the top of the
+  // iteration
+  int32_t nbn[C::FPT];
+  auto load_nbr = [&](int64_t g, int32_t *dst) {
+#pragma unroll
+    for (int u = 0; u < C::FPT; ++u) {
+      const int fs = tid + u * C::THREADS;
+      const int el = fs / (NF * Nfp), f = (fs / Nfp) % NF;
+      const int64_t e = g * EPB + el;
+      dst[u] = (g < ngroups && fs < C::FSLOTS && e < nelem) ? nbr[f + NF * e] : NBR_WALL;
+    }
+  };
+  load_nbr(blockIdx.x, nbn);
+
+  bool bad = false, timed_out = false;
   int it = 0;
   for (int64_t g = blockIdx.x; g < ngroups; g += gridDim.x, ++it) {
     const int b = it & 1;
@@ -183,17 +272,18 @@ k_stage_pipe(const T *__restrict__ Qin, T *__restrict__ Qout, T *__restrict__ rh
     T qP[C::FPT][NS], nrm[C::FPT][DIM], smj[C::FPT];
     int32_t nbv[C::FPT];
 #pragma unroll
+    for (int u = 0; u < C::FPT; ++u) nbv[u] = nbn[u];
+    load_nbr(gn, nbn);
+#pragma unroll
     for (int u = 0; u < C::FPT; ++u) {
       const int fs = tid + u * C::THREADS;
       const int el = fs / (NF * Nfp), f = (fs / Nfp) % NF, fn = fs % Nfp;
       const int64_t e = e0 + el;
-      nbv[u] = NBR_WALL;
       if (fs < C::FSLOTS && e < nelem) {
         const T *sg = sgeo + (int64_t)NSG * (fn + (int64_t)Nfp * (f + NF * e));
 #pragma unroll
         for (int c = 0; c < DIM; ++c) nrm[u][c] = sg[c];
         smj[u] = sg[DIM];
-        nbv[u] = nbr[f + NF * e];
         if (nbv[u] >= 0) {
           const int64_t e2 = nbv[u] >> 3;
           const int vP = face_node<DIM, Nq>(nbv[u] & 7, fn);
@@ -203,27 +293,23 @@ k_stage_pipe(const T *__restrict__ Qin, T *__restrict__ Qout, T *__restrict__ rh
       }
     }
 
-    // ---- wait for this group's slabs
-    bool ok = true;
+    // ---- wait for this group's slabs (each thread observes the mbarrier; a
+    // wait that gives up flags the status word and the iteration continues)
     if constexpr (PP::BULK) {
-      ok = mbar_wait_bounded(&bars[b], (uint32_t)((it >> 1) & 1), WAIT_LIMIT);
+      if (!mbar_wait_bounded(&bars[b], (uint32_t)((it >> 1) & 1), WAIT_LIMIT)) timed_out = true;
     } else {
       cp_async_wait<1>();
+      __syncthreads();
     }
-    if (__syncthreads_or(!ok)) {
-      if (tid == 0) atomicOr(status, ST_TIMEOUT);
-      if constexpr (PP::BULK) {
-        if (gn < ngroups) mbar_wait_bounded(&bars[b ^ 1], (uint32_t)(((it + 1) >> 1) & 1), WAIT_LIMIT);
-      }
-      return;
-    }
-    const T *Qs = sQ(b), *Gs = sG(b);
+    const T *Qs = stage0 + b * STRIDE, *Gs = Qs + EPB * Np * NS;
 
-    // ---- pointwise fluxes
+    // ---- phase A: contravariant volume fluxes and face fluxes
+    T buoy[C::NPT];
 #pragma unroll
     for (int u = 0; u < C::NPT; ++u) {
       const int slot = tid + u * C::THREADS;
       const int el = slot / Np, n = slot % Np;
+      buoy[u] = T(0);
       if (slot < SP && e0 + el < nelem) {
         T q[NS];
 #pragma unroll
@@ -235,30 +321,26 @@ k_stage_pipe(const T *__restrict__ Qin, T *__restrict__ Qout, T *__restrict__ rh
           for (int c = 0; c < DIM; ++c) met[r][c] = Gs[(el * NG + r + DIM * c) * Np + n];
         const T MJ = Gs[(el * NG + DIM * DIM) * Np + n];
         const T gc = p.grav != T(0) ? vgeo[n + Np * (GC + NVG * (e0 + el))] : T(0);
-        const T P = pressure<DIM, T>(q, gc, p);
+        const T ri = T(1) / q[IR];
+        const T P = pressure_ri<DIM, T>(q, ri, gc, p);
         T f[NS][DIM];
-        euler_flux<DIM, T>(q, P, f);
+        euler_flux_ri<DIM, T>(q, ri, P, f);
+        const int i = n % Nq, j = (n / Nq) % Nq, k = DIM == 3 ? n / (Nq * Nq) : 0;
 #pragma unroll
-        for (int r = 0; r < DIM; ++r)
+        for (int r = 0; r < DIM; ++r) {
+          // row of this node in direction r and its position along the row
+          const int row = DIM == 2 ? (r == 0 ? j : i) : (r == 0 ? j + Nq * k : (r == 1 ? i + Nq * k : i + Nq * j));
+          const int pos = r == 0 ? i : (r == 1 ? j : k);
 #pragma unroll
           for (int s = 0; s < NS; ++s) {
             T a = met[r][0] * f[s][0] + met[r][1] * f[s][1];
             if (DIM == 3) a = a + met[r][2] * f[s][2];
-            sF[(r * NS + s) * SP + slot] = MJ * a;
+            sF[r * PP::FDIR + ((size_t)(s * EPB + el) * NR + row) * RS + pos] = MJ * a;
           }
-        R[u][DIM - 1] -= MJ * q[Lay<DIM>::IR] * p.grav;
+        }
+        buoy[u] = MJ * q[IR] * p.grav;
       }
     }
-    __syncthreads();
-    // ---- volume contraction
-#pragma unroll
-    for (int u = 0; u < C::NPT; ++u) {
-      const int slot = tid + u * C::THREADS;
-      const int el = slot / Np, n = slot % Np;
-      if (slot < SP && e0 + el < nelem) contract<DIM, Nq, EPB, T>(sF, Ds, el, n, R[u]);
-    }
-    __syncthreads();
-    // ---- face fluxes
 #pragma unroll
     for (int u = 0; u < C::FPT; ++u) {
       const int fs = tid + u * C::THREADS;
@@ -269,8 +351,9 @@ k_stage_pipe(const T *__restrict__ Qin, T *__restrict__ Qout, T *__restrict__ rh
 #pragma unroll
         for (int s = 0; s < NS; ++s) qM[s] = Qs[(el * NS + s) * Np + vM] + qref.v[s];
         const T gM = p.grav != T(0) ? vgeo[vM + Np * (GC + NVG * (e0 + el))] : T(0);
-        const T PM = pressure<DIM, T>(qM, gM, p);
-        T PPv;
+        const T riM = T(1) / qM[IR];
+        const T PM = pressure_ri<DIM, T>(qM, riM, gM, p);
+        T PPv, riP;
         if (nbv[u] >= 0) {
 #pragma unroll
           for (int s = 0; s < NS; ++s) qq[s] = qP[u][s];
@@ -279,25 +362,29 @@ k_stage_pipe(const T *__restrict__ Qin, T *__restrict__ Qout, T *__restrict__ rh
             const int64_t e2 = nbv[u] >> 3;
             gP = vgeo[face_node<DIM, Nq>(nbv[u] & 7, fn) + Np * (GC + NVG * e2)];
           }
-          PPv = pressure<DIM, T>(qq, gP, p);
+          riP = T(1) / qq[IR];
+          PPv = pressure_ri<DIM, T>(qq, riP, gP, p);
         } else {
           wall_state<DIM, T>(qM, nrm[u], qq);
+          riP = riM;
           PPv = PM;
         }
         T out[NS];
-        rusanov<DIM, T>(qM, PM, qq, PPv, nrm[u], p, out);
+        rusanov_n<DIM, T>(qM, riM, PM, qq, riP, PPv, nrm[u], p, out);
 #pragma unroll
         for (int s = 0; s < NS; ++s) FF[(f * NS + s) * FS + el * Nfp + fn] = smj[u] * out[s];
       }
     }
     __syncthreads();
-    // ---- face accumulation and LSRK update
+    // ---- phase B: carry - source + volume contraction - face terms, update
 #pragma unroll
     for (int u = 0; u < C::NPT; ++u) {
       const int slot = tid + u * C::THREADS;
       const int el = slot / Np, n = slot % Np;
       const int64_t e = e0 + el;
       if (slot < SP && e < nelem) {
+        R[u][DIM - 1] -= buoy[u];
+        contract_rows<DIM, Nq, T>(sF, DT, el, n, R[u]);
         gather_face_terms<DIM, Nq, EPB, T>(FF, el, n, R[u]);
         const T mji = Gs[(el * NG + MJI) * Np + n];
 #pragma unroll
@@ -309,10 +396,11 @@ k_stage_pipe(const T *__restrict__ Qin, T *__restrict__ Qout, T *__restrict__ rh
         }
       }
     }
-    __syncthreads();  // stage b and FF are free for the next iterations
+    __syncthreads();  // stage b, the flux rows and FF are free for reuse
   }
   if constexpr (!PP::BULK) cp_async_wait<0>();
   if (bad) atomicOr(status, ST_NONFINITE);
+  if (timed_out) atomicOr(status, ST_TIMEOUT);
 }
 
 }  // namespace cb

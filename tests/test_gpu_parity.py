@@ -152,7 +152,7 @@ def test_fused_lsrk_vortex_500_steps():
     s.close()
 
 
-@pytest.mark.parametrize("N,n,nsteps", [(7, 4, 1), (7, 4, 7), (7, 8, 4), (4, 6, 3), (3, 6, 2), (10, 2, 2)])
+@pytest.mark.parametrize("N,n,nsteps", [(7, 4, 1), (7, 4, 7), (7, 8, 4), (4, 8, 2), (3, 6, 2), (10, 2, 2)])
 def test_fused_lsrk_3d_warped(N, n, nsteps):
     """Fused driver on warped periodic cubes; n=8 at N=7 gives more elements
     than SMs so every block runs several pipelined iterations; N=4 and N=3
