@@ -272,11 +272,8 @@ def main():
     if tdist is not None:
         tdist.barrier()
     clk = clocks.stop()
-    t_ms = e0.elapsed_time(e1)
-    if tdist is not None:
-        tt = torch.tensor([t_ms], dtype=torch.float64, device=dev)
-        tdist.all_reduce(tt, op=tdist.ReduceOp.MAX)
-        t_ms = float(tt.item())
+    from canary_b200 import replicas
+    t_ms = replicas.max_over_ranks(e0.elapsed_time(e1), device=dev)
     sums = solver.sums()
     finite = bool(np.all(np.isfinite(sums)))
 
@@ -300,11 +297,7 @@ def main():
         hout.copy_(dQ, non_blocking=True)
     f1.record(stream)
     torch.cuda.synchronize(dev)
-    e2e_ms = f0.elapsed_time(f1)
-    if tdist is not None:
-        tt = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
-        tdist.all_reduce(tt, op=tdist.ReduceOp.MAX)
-        e2e_ms = float(tt.item())
+    e2e_ms = replicas.max_over_ranks(f0.elapsed_time(f1), device=dev)
     solver.close()
 
     w = 8 if args.precision == 64 else 4

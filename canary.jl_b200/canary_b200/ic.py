@@ -64,19 +64,26 @@ def fourier_state(x, y, z, seed=0, kmax=4, gamma=GAMMA, device=None, dtype=None)
     """Conserved (U, V, W, ρ, E) of the random Fourier state with p = 1:
     ρ = 1 + Σ a_k sin(k·x + φ_k), (u, v, w) = Σ a_k sin(k·x + φ_k).
 
-    Evaluated with torch on `device` (e.g. "cuda") when given, else numpy;
-    both use float64 and the same summation order."""
+    Evaluated in float64 with torch on `device` (e.g. "cuda") when given,
+    summing 16 wave vectors per batch, else with numpy one wave vector at a
+    time; the two orders of summation agree to round-off."""
     ks, coef = fourier_coefficients(seed, kmax)
     if device is not None:
         import torch
-        X = [torch.as_tensor(np.asarray(c), dtype=torch.float64, device=device) for c in (x, y, z)]
+        X = [torch.as_tensor(np.asarray(c), dtype=torch.float64, device=device).reshape(-1)
+             for c in (x, y, z)]
+        K = torch.as_tensor(ks, dtype=torch.float64, device=device)
         out = []
-        for fi, (a, phi) in enumerate(coef):
+        chunk = 16
+        for a, phi in coef:
+            A = torch.as_tensor(a, dtype=torch.float64, device=device)
+            PH = torch.as_tensor(phi, dtype=torch.float64, device=device)
             acc = torch.zeros_like(X[0])
-            for q in range(len(ks)):
-                arg = (ks[q, 0] * X[0] + ks[q, 1] * X[1]) + ks[q, 2] * X[2] + phi[q]
-                acc = acc + a[q] * torch.sin(arg)
-            out.append(acc)
+            for q0 in range(0, len(ks), chunk):
+                sl = slice(q0, min(q0 + chunk, len(ks)))
+                arg = (K[sl, 0:1] * X[0] + K[sl, 1:2] * X[1]) + K[sl, 2:3] * X[2] + PH[sl, None]
+                acc = acc + (A[sl, None] * torch.sin(arg)).sum(0)
+            out.append(acc.reshape(np.shape(x)))
         rho = 1.0 + out[0]
         u, v, w = out[1], out[2], out[3]
         E = 1.0 / (gamma - 1.0) + 0.5 * rho * (u * u + v * v + w * w)
