@@ -24,7 +24,7 @@ EXPORTS = (
     "cb_updatesolution", "cb_updatesolution_f32",
     "cb_volume_grad", "cb_flux_grad", "cb_update_gradQ", "cb_volume_div", "cb_flux_div",
     "cb_solver_create", "cb_lsrk_run", "cb_solver_set_offset", "cb_solver_sums",
-    "cb_solver_destroy",
+    "cb_solver_destroy", "cb_lsrk_stage_noalloc",
 )
 
 
@@ -77,6 +77,8 @@ def lib() -> C.CDLL:
     L.cb_solver_sums.argtypes = [vp, C.POINTER(C.c_double)]
     L.cb_solver_set_offset.argtypes = [vp, C.POINTER(C.c_double)]
     L.cb_solver_destroy.argtypes = [vp]
+    L.cb_lsrk_stage_noalloc.argtypes = [C.c_int, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp, i64,
+                                        phys_p, dbl, dbl, dbl, vp, vp]
     _lib = L
     return L
 

@@ -179,6 +179,28 @@ def flux_div(dim, N, rhs, gradQ, Q, sgeo, elems, vmapM, vmapP, elemtobndy, phys=
                                  _stream(stream)))
 
 
+NOALLOC_SCRATCH_BYTES = 32 * 1024 * 1024  # CB_NOALLOC_SCRATCH_BYTES
+
+
+def lsrk_stage_noalloc(dim, N, Q, rhs, vgeo, sgeo, vmapM, vmapP, elemtobndy, D, elems, rka,
+                       rkb, dt, phys=None, status=None, stream=None):
+    """One fused FP64 LSRK stage without any device allocation (for hosts
+    that own every device allocation): same result as volumerhs, fluxrhs and
+    updatesolution in sequence.  Its scratch is a fixed static device array
+    shared by all calls, so calls must not overlap on the GPU.  `status`, if
+    given, is a CUDA int32 tensor that receives the kernel status bits."""
+    torch = _torch()
+    n = _nelem(elems)
+    Np, Nfp, nf = _sizes(dim, N, n)
+    ns = nstate(dim)
+    check(_lib.lib().cb_lsrk_stage_noalloc(
+        dim, N, _ptr(Q, torch.float64, Np * ns * n, "Q"), _ptr(rhs, torch.float64, Np * ns * n, "rhs"),
+        _ptr(vgeo, torch.float64), _ptr(sgeo, torch.float64), _ptr(vmapM, torch.int64),
+        _ptr(vmapP, torch.int64), _ptr(elemtobndy, torch.int64), _ptr(D, torch.float64), n,
+        C.byref(phys or make_phys()), float(rka), float(rkb), float(dt),
+        _ptr(status, torch.int32) if status is not None else None, _stream(stream)))
+
+
 def device_status(stream=None) -> None:
     """Synchronise and raise if a kernel met an invalid boundary code or a
     non-finite state since the last check."""

@@ -182,6 +182,42 @@ int cb_solver_set_offset(cb_solver *s, const double *qref);
 int cb_solver_sums(cb_solver *s, double *out_host);
 int cb_solver_destroy(cb_solver *s);
 
+/* ---------------------------------------------------------------------- */
+/* Allocation-free stage (no counterpart in the reference).                */
+/* ---------------------------------------------------------------------- */
+
+/* Size of the file-scope device array that cb_lsrk_stage_noalloc uses as
+ * scratch; every GPU that loads the library holds it until the process
+ * exits. */
+#define CB_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
+
+/* One LSRK(5,4) stage, FP64, for callers that cannot allocate device memory
+ * (an embedding whose host runtime owns every device allocation, or a path
+ * where an allocation's implicit synchronisation is not allowed).  It has no
+ * counterpart in the reference.  Same result as cb_volumerhs, cb_fluxrhs and
+ * cb_updatesolution(rhs_gradQ = NULL, visc = 0) called in that order with the
+ * same rka, rkb, dt; Q and rhs are updated in place.
+ *
+ * It calls no cudaMalloc/cudaFree and no allocating library routine: its
+ * scratch (a copy of the stage's input state, the face-neighbour table and a
+ * status word) lives in a static device array of CB_NOALLOC_SCRATCH_BYTES.
+ * A mesh whose scratch need (about 8·Np·nstate + 4·2·dim bytes per element)
+ * exceeds it is rejected with CB_ERR_ARG before any device work.  The first
+ * call on a device looks up the array's device address (once per device, with
+ * that device current); make that first call before any stream capture.
+ * Every call shares the one array, so calls that overlap on the GPU (other
+ * streams, other host threads) race; serialise them.  Kernel-detected
+ * problems (boundary code other than 0/1, vmaps that are not a conforming
+ * mesh, non-finite state) are OR-ed into *status when status is a non-NULL
+ * device pointer (the caller clears it). */
+int cb_lsrk_stage_noalloc(int dim, int N, double *Q, double *rhs,
+                          const double *vgeo, const double *sgeo,
+                          const int64_t *vmapM, const int64_t *vmapP,
+                          const int64_t *elemtobndy, const double *D,
+                          int64_t nelem, const cb_phys *phys, double rka,
+                          double rkb, double dt, unsigned *status,
+                          cb_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif
