@@ -755,6 +755,7 @@ __global__ void k_round_f32(float *__restrict__ dst, const double *__restrict__ 
 
 }  // namespace cb
 #include "cb_pipe.cuh"
+#include "cb_pipe2.cuh"
 namespace cb {
 
 // ---------------------------------------------------------------- launchers
@@ -798,7 +799,19 @@ struct Launch {
                            cudaStream_t st) {
     constexpr bool pipe_ok = Pipe<DIM, Nq, T>::OK;
     const bool aligned = ((reinterpret_cast<uintptr_t>(Qin) | reinterpret_cast<uintptr_t>(vgeo)) & 15) == 0;
-    if (pipe_ok && aligned) {
+    const bool aligned2 = aligned && ((reinterpret_cast<uintptr_t>(rhs) | reinterpret_cast<uintptr_t>(sgeo)) & 15) == 0;
+    if (Pipe2<DIM, Nq, T>::OK && aligned2) {
+      using PP = Pipe2<DIM, Nq, T>;
+      size_t sm = PP::smem();
+      cudaError_t err = prep(k_stage_pipe2<DIM, Nq, T>, sm);
+      if (err != cudaSuccess) return err;
+      const int64_t groups = (nelem + C::EPB - 1) / C::EPB;
+      int g = num_sms();
+      if ((int64_t)g > groups) g = (int)groups;
+      k_stage_pipe2<DIM, Nq, T><<<g, C::THREADS, sm, st>>>(Qin, Qout, rhs, vgeo, sgeo, nbr, D, nelem,
+                                                           p, qref, rka, rkbdt, status);
+      return cudaGetLastError();
+    } else if (pipe_ok && aligned) {
       using PP = Pipe<DIM, Nq, T>;
       size_t sm = PP::smem();
       cudaError_t err = prep(k_stage_pipe<DIM, Nq, T>, sm);
