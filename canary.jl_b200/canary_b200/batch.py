@@ -1,0 +1,276 @@
+"""Batched LSRK(5,4) over many independent DG instances (cb_mesh_* and
+cb_batch_* of include/canary_b200.h).
+
+The reference advances one mesh per `lowstorageRK` call
+(euler2d_set3c.jl:1109-1282, euler3d_set3c.jl:1361-1523); a `Batch` advances
+many instances of uneven order and size in one graph launch per step, each
+with its own dt, step count and state, and admits and releases instances
+between runs (continuous batching).  An instance's result does not depend on
+what else is in the batch.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import check
+from .dg import DeviceMesh, _ptr, _stream, _torch, from_device, make_phys, nstate, to_device
+
+MAX_ORDER = {2: 8, 3: 7}  # orders compiled into the batched stage
+
+
+class BatchMesh:
+    """Geometry and face-neighbour table shared by all batch instances on one
+    mesh (cb_mesh): the FP64 device arrays of `dmesh` for precision 64, rounded
+    FP32 copies for precision 32.  Keep it alive while instances use it."""
+
+    def __init__(self, dmesh: DeviceMesh, precision: int = 64, stream=None):
+        torch = _torch()
+        m = dmesh.mesh
+        self.dmesh, self.precision = dmesh, precision
+        self.dim, self.N, self.nelem = m.dim, m.N, m.nelem
+        self._h = C.c_void_p()
+        check(_lib.lib().cb_mesh_create(
+            C.byref(self._h), m.dim, m.N, precision, m.nelem, _ptr(dmesh.vgeo, torch.float64),
+            _ptr(dmesh.sgeo, torch.float64), _ptr(dmesh.vmapM, torch.int64), _ptr(dmesh.vmapP, torch.int64),
+            _ptr(dmesh.elemtobndy, torch.int64), _ptr(dmesh.D, torch.float64), _stream(stream)))
+
+    @property
+    def Np(self) -> int:
+        return (self.N + 1) ** self.dim
+
+    def close(self) -> None:
+        if self._h:
+            _lib.lib().cb_mesh_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """A batch of up to `max_instances` slots (cb_batch).  All work is ordered
+    on `stream` (the current torch stream by default)."""
+
+    def __init__(self, precision: int = 64, max_instances: int = 1024, phys=None, stream=None):
+        self.precision = precision
+        self.max_instances = max_instances
+        self.phys = phys or make_phys()
+        self._h = C.c_void_p()
+        check(_lib.lib().cb_batch_create(C.byref(self._h), precision, max_instances, C.byref(self.phys),
+                                         _stream(stream)))
+        self._inst = {}  # slot -> (mesh, Q, rhs, offset)
+
+    def set_variant(self, dim: int, N: int, variant: int) -> None:
+        """Group shape for instances of (dim, N) admitted from now on
+        (0: ~256 nodes per block, 1: ~512)."""
+        check(_lib.lib().cb_batch_set_variant(self._h, dim, N, variant))
+
+    def add(self, mesh: BatchMesh, Q, rhs, dt: float, nsteps: int, qref=None) -> int:
+        """Admit the caller's device state Q and zeroed carry rhs (flat tensors
+        of the batch precision); returns the slot."""
+        torch = _torch()
+        real = torch.float64 if self.precision == 64 else torch.float32
+        n = mesh.nelem * mesh.Np * nstate(mesh.dim)
+        ns = nstate(mesh.dim)
+        off = np.zeros(ns) if qref is None else np.asarray(qref, dtype=np.float64)[:ns]
+        arr = (C.c_double * 5)(*([float(v) for v in off] + [0.0] * (5 - ns)))
+        slot = C.c_int(-1)
+        check(_lib.lib().cb_batch_add(self._h, mesh._h, _ptr(Q, real, n, "Q"), _ptr(rhs, real, n, "rhs"),
+                                      float(dt), int(nsteps), arr, C.byref(slot)))
+        self._inst[slot.value] = (mesh, Q, rhs, off)
+        return slot.value
+
+    def add_state(self, mesh: BatchMesh, Q: np.ndarray, dt: float, nsteps: int, offset=None) -> int:
+        """Admit a host state Q (Np, nstate, nelem).  For precision 32 the
+        device state holds Q - qref with qref = per-field mean of Q (unless
+        `offset` is given); `result` returns the full FP64 state."""
+        torch = _torch()
+        Q = np.asarray(Q, dtype=np.float64)
+        if offset is None:
+            offset = Q.mean(axis=(0, 2)) if self.precision == 32 else np.zeros(Q.shape[1])
+        offset = np.asarray(offset, dtype=np.float64)
+        real = torch.float64 if self.precision == 64 else torch.float32
+        dQ = to_device(Q - offset[None, :, None], real, mesh.dmesh.vgeo.device)
+        return self.add(mesh, dQ, torch.zeros_like(dQ), dt, nsteps, offset)
+
+    def run(self, nsteps: int) -> None:
+        """Advance every admitted instance by nsteps steps (each stops at its
+        own step count)."""
+        check(_lib.lib().cb_batch_run(self._h, int(nsteps)))
+
+    def info(self, slot: int) -> tuple[int, int]:
+        """(steps taken, steps to take) of a slot."""
+        done, target = C.c_int64(), C.c_int64()
+        check(_lib.lib().cb_batch_info(self._h, slot, C.byref(done), C.byref(target)))
+        return done.value, target.value
+
+    def release(self, slot: int):
+        """Retire a slot; its final state is placed in the caller's Q.
+        Returns (Q, rhs) tensors."""
+        check(_lib.lib().cb_batch_release(self._h, slot))
+        mesh, Q, rhs, off = self._inst.pop(slot)
+        return Q, rhs
+
+    def result(self, slot: int) -> np.ndarray:
+        """Retire a slot admitted by `add_state` and return its full FP64
+        state (Np, nstate, nelem) on the host."""
+        mesh, _, _, off = self._inst[slot]
+        Q, _ = self.release(slot)
+        shape = (mesh.Np, nstate(mesh.dim), mesh.nelem)
+        return from_device(Q.double(), shape) + off[None, :, None]
+
+    def status(self) -> np.ndarray:
+        """Per-slot sticky status bits (bit 2: non-finite state); synchronises."""
+        out = (C.c_uint * self.max_instances)()
+        check(_lib.lib().cb_batch_status(self._h, out))
+        return np.array(out[:], dtype=np.uint32)
+
+    def close(self) -> None:
+        if self._h:
+            _lib.lib().cb_batch_destroy(self._h)
+            self._h = C.c_void_p()
+            self._inst.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------------------ ensembles
+class MeshCache:
+    """Host meshes, device geometry and batch meshes shared by all instances
+    with the same (dim, N, n_side) (the geometry does not depend on the
+    initial state)."""
+
+    def __init__(self, device="cuda"):
+        self.device = device
+        self._host, self._dev, self._batch = {}, {}, {}
+
+    def host(self, dim: int, N: int, n_side: int, L: float = 10.0, warp=None):
+        from .dg import build_mesh
+        key = (dim, N, n_side, L, warp is not None)
+        if key not in self._host:
+            x = (np.linspace(0.0, L, n_side + 1),) * dim
+            self._host[key] = build_mesh(dim, N, x, (True,) * dim, meshwarp=warp)
+        return self._host[key]
+
+    def batch_mesh(self, precision: int, dim: int, N: int, n_side: int, L: float = 10.0, warp=None):
+        key = (precision, dim, N, n_side, L, warp is not None)
+        if key not in self._batch:
+            hkey = key[1:]
+            if hkey not in self._dev:
+                self._dev[hkey] = DeviceMesh.upload(self.host(dim, N, n_side, L, warp), self.device)
+            self._batch[key] = BatchMesh(self._dev[hkey], precision)
+        return self._batch[key]
+
+    def close(self) -> None:
+        for bm in self._batch.values():
+            bm.close()
+        self._batch.clear()
+        self._dev.clear()
+
+
+def vortex_state(mesh, beta: float, xc: float, yc: float) -> np.ndarray:
+    """Conserved (U, V, ρ, E) of the isentropic vortex on a 2-D mesh."""
+    from .ic import isentropic_vortex
+    x, y = mesh.coords()
+    U, V, rho, E = isentropic_vortex(x, y, beta, xc, yc)
+    Q = np.empty((mesh.Np, 4, mesh.nelem), order="F")
+    Q[:, 0], Q[:, 1], Q[:, 2], Q[:, 3] = U, V, rho, E
+    return Q
+
+
+class VortexEnsemble:
+    """Independent 2-D isentropic-vortex instances (parameters from
+    ic.vortex_ensemble) advancing together in one Batch.  For precision 32
+    each instance stores its deviation from the free stream (U, V, ρ, E) =
+    (1, 0, 1, 1/(γ-1) + 1/2)."""
+
+    FREE_STREAM = (1.0, 0.0, 1.0, 1.0 / 0.4 + 0.5)
+
+    def __init__(self, params, precision=64, dt=0.002, nsteps=500, phys=None, tuning=None, cache=None):
+        self.params, self.precision, self.dt, self.nsteps = list(params), precision, dt, nsteps
+        self.cache = cache or MeshCache()
+        self.batch = Batch(precision, max_instances=max(len(self.params), 1), phys=phys)
+        for (dim, N), v in (tuning or {}).items():
+            self.batch.set_variant(dim, N, v)
+        off = np.array(self.FREE_STREAM) if precision == 32 else np.zeros(4)
+        self.slots = []
+        self.nodes = 0
+        for p in self.params:
+            bm = self.cache.batch_mesh(precision, 2, p["N"], p["n_side"])
+            Q = vortex_state(self.cache.host(2, p["N"], p["n_side"]), p["beta"], p["xc"], p["yc"])
+            self.slots.append(self.batch.add_state(bm, Q, dt, nsteps, off))
+            self.nodes += bm.Np * bm.nelem
+
+    @property
+    def dof(self) -> int:
+        return 4 * self.nodes
+
+    def run(self, nsteps=None) -> None:
+        self.batch.run(self.nsteps if nsteps is None else nsteps)
+
+    def results(self):
+        """Retire every instance; final FP64 host states in parameter order."""
+        return [self.batch.result(s) for s in self.slots]
+
+    def close(self) -> None:
+        self.batch.close()
+
+
+# ------------------------------------------------------------------ autotuner
+def autotune(precision: int, shapes, nodes_target: int = 4_000_000, steps: int = 4, repeat: int = 3,
+             stream=None) -> dict:
+    """Choose the element-group variant (elements per block) of each (dim, N)
+    by timing the batched step on a synthetic instance of that shape with
+    about `nodes_target` nodes: 2-D vortex / 3-D free-stream-plus-Fourier
+    states on periodic meshes.  Returns {(dim, N): variant}."""
+    torch = _torch()
+    from .ic import fourier_state
+    best = {}
+    for dim, N in shapes:
+        Np = (N + 1) ** dim
+        n_side = max(2, int(round((nodes_target / Np) ** (1.0 / dim))))
+        L = 10.0 if dim == 2 else 2 * np.pi
+        cache = MeshCache()
+        mesh = cache.host(dim, N, n_side, L)
+        if dim == 2:
+            Q = vortex_state(mesh, 5.0, 5.0, 5.0)
+            dt = 1e-4
+        else:
+            x, y, z = mesh.coords()
+            Q = np.stack(fourier_state(x, y, z, seed=0, device="cuda"), axis=1)
+            dt = 1e-5
+        timings = {}
+        for var in (0, 1):
+            b = Batch(precision, 1)
+            try:
+                b.set_variant(dim, N, var)
+            except Exception:
+                b.close()
+                continue
+            slot = b.add_state(cache.batch_mesh(precision, dim, N, n_side, L), Q, dt, 10 ** 9)
+            b.run(1)  # build the graph, warm up
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ts = []
+            for _ in range(repeat):
+                torch.cuda.synchronize()
+                ev0.record()
+                b.run(steps)
+                ev1.record()
+                torch.cuda.synchronize()
+                ts.append(ev0.elapsed_time(ev1))
+            timings[var] = min(ts)
+            b.release(slot)
+            b.close()
+        cache.close()
+        best[(dim, N)] = min(timings, key=timings.get)
+    return best

@@ -118,3 +118,20 @@ def max_wave_speed(Q, dim, gamma=GAMMA):
 def fourier_dt(Q, N, h=2 * math.pi / 32, gamma=GAMMA):
     """dt = 0.2 h / (N^2 max(|u| + c))."""
     return 0.2 * h / (N * N * max_wave_speed(Q, 3, gamma))
+
+
+def vortex_ensemble(count: int = 512, seed: int = 0):
+    """Parameters of an ensemble of independent 2-D vortex instances on
+    [0,10]^2: instance i draws, from numpy's PCG64(seed + i) in this order,
+    N ~ U{3..8}, elements per side ~ U{4..48}, β ~ U(1,5) and the centre
+    (xc, yc) ~ U([2,8]^2).  Every other setting is that of the single vortex
+    (free stream ρ=1, u=1, v=0, p=1, dt=0.002, 500 steps)."""
+    out = []
+    for i in range(count):
+        rng = np.random.Generator(np.random.PCG64(seed + i))
+        N = int(rng.integers(3, 9))
+        n_side = int(rng.integers(4, 49))
+        beta = float(rng.uniform(1.0, 5.0))
+        xc, yc = (float(v) for v in rng.uniform(2.0, 8.0, 2))
+        out.append(dict(N=N, n_side=n_side, beta=beta, xc=xc, yc=yc))
+    return out

@@ -183,6 +183,63 @@ int cb_solver_sums(cb_solver *s, double *out_host);
 int cb_solver_destroy(cb_solver *s);
 
 /* ---------------------------------------------------------------------- */
+/* Batched LSRK(5,4) over many independent instances (ensembles, serving). */
+/* ---------------------------------------------------------------------- */
+
+/* The reference advances one mesh per lowstorageRK call
+ * (euler2d_set3c.jl:1109-1282); a batch advances many independent instances
+ * of uneven order and element count together, each with its own dt, step
+ * count and state, with the same per-instance result as cb_lsrk_run (the
+ * fused stage arithmetic is the same; results do not depend on what else is
+ * in the batch).  Inviscid form, dim 2 with N 1..8 and dim 3 with N 1..7.
+ *
+ * A cb_mesh holds what instances on the same mesh share: the geometry (the
+ * caller's FP64 arrays for precision 64, rounded FP32 copies for precision 32)
+ * and the int32 face-neighbour table built from vmapM/vmapP/elemtobndy.  It
+ * validates the vmaps (CB_ERR_MESH, CB_ERR_BC) and synchronises `stream`.  A
+ * mesh must outlive the batch instances that use it. */
+typedef struct cb_mesh cb_mesh;
+int cb_mesh_create(cb_mesh **out, int dim, int N, int precision,
+                   int64_t nelem, const double *vgeo, const double *sgeo,
+                   const int64_t *vmapM, const int64_t *vmapP,
+                   const int64_t *elemtobndy, const double *D,
+                   cb_stream_t stream);
+int cb_mesh_destroy(cb_mesh *m);
+
+/* A batch of up to max_instances slots.  All calls are ordered on `stream`
+ * (0: the batch makes its own) and asynchronous except cb_batch_status and
+ * cb_batch_destroy.  visc must be 0. */
+typedef struct cb_batch cb_batch;
+int cb_batch_create(cb_batch **out, int precision, int max_instances,
+                    const cb_phys *phys, cb_stream_t stream);
+/* Element-group shape used for instances of (dim, N) admitted from now on:
+ * variant 0 groups about 256 nodes per block, variant 1 about 512
+ * (CB_ERR_UNSUPPORTED where it would need more than two nodes per thread).
+ * Chosen by an autotuner; the results do not depend on it. */
+int cb_batch_set_variant(cb_batch *b, int dim, int N, int variant);
+/* Admit an instance: the caller's state Q and zeroed residual carry rhs
+ * (layouts as above, precision of the batch) advance by nsteps steps of dt
+ * during the following cb_batch_run calls.  qref (nstate doubles, or NULL for
+ * zeros) are per-field offsets as in cb_solver_set_offset (Q holds Q - qref).
+ * Writes the slot id.  The batch keeps a twin state buffer from its own
+ * stream-ordered pool. */
+int cb_batch_add(cb_batch *b, const cb_mesh *m, void *Q, void *rhs, double dt,
+                 int64_t nsteps, const double *qref, int *slot);
+/* Advance every admitted instance by nsteps steps, each stopping at its own
+ * step count; one captured CUDA graph per step (5 stage launches per
+ * dimension present, 2-D and 3-D in concurrent branches). */
+int cb_batch_run(cb_batch *b, int64_t nsteps);
+/* Steps taken and to take by a slot (host bookkeeping, no synchronisation). */
+int cb_batch_info(const cb_batch *b, int slot, int64_t *done, int64_t *target);
+/* Retire a slot: the instance's current state is placed in its Q (stream-
+ * ordered), the twin buffer returns to the pool and the slot is free. */
+int cb_batch_release(cb_batch *b, int slot);
+/* Per-slot sticky status bits (out_host[max_instances]; bit 2 = non-finite
+ * state); synchronises. */
+int cb_batch_status(cb_batch *b, unsigned *out_host);
+int cb_batch_destroy(cb_batch *b);
+
+/* ---------------------------------------------------------------------- */
 /* Allocation-free stage (no counterpart in the reference).                */
 /* ---------------------------------------------------------------------- */
 

@@ -58,3 +58,31 @@ def test_check_raises():
         L = _lib.lib()
         phys = _lib.cb_phys(1.4, 1.0, 3.5, 2.5, 0.0, 0.72, -2 / 3, 0.0)
         _lib.check(L.cb_volumerhs(5, 3, None, None, None, None, 1, C.byref(phys), None))
+
+
+def test_batch_argument_validation_without_device():
+    L = _lib.lib()
+    phys = _lib.cb_phys(1.4, 1.0, 3.5, 2.5, 0.0, 0.72, -2 / 3, 0.0)
+    visc = _lib.cb_phys(1.4, 1.0, 3.5, 2.5, 0.0, 0.72, -2 / 3, 1e-3)
+    dummy = C.c_void_p(16)
+    h = C.c_void_p()
+    # orders outside the batched range, bad dim / precision, null arrays
+    assert L.cb_mesh_create(C.byref(h), 2, 9, 64, 4, dummy, dummy, dummy, dummy, dummy, dummy,
+                            None) == _lib.CB_ERR_UNSUPPORTED
+    assert L.cb_mesh_create(C.byref(h), 3, 8, 64, 4, dummy, dummy, dummy, dummy, dummy, dummy,
+                            None) == _lib.CB_ERR_UNSUPPORTED
+    assert L.cb_mesh_create(C.byref(h), 4, 3, 64, 4, dummy, dummy, dummy, dummy, dummy, dummy,
+                            None) == _lib.CB_ERR_ARG
+    assert L.cb_mesh_create(C.byref(h), 2, 3, 16, 4, dummy, dummy, dummy, dummy, dummy, dummy,
+                            None) == _lib.CB_ERR_ARG
+    assert L.cb_mesh_create(C.byref(h), 2, 3, 64, 4, None, dummy, dummy, dummy, dummy, dummy,
+                            None) == _lib.CB_ERR_ARG
+    assert L.cb_batch_create(C.byref(h), 16, 8, C.byref(phys), None) == _lib.CB_ERR_ARG
+    assert L.cb_batch_create(C.byref(h), 64, 0, C.byref(phys), None) == _lib.CB_ERR_ARG
+    assert L.cb_batch_create(C.byref(h), 64, 8, C.byref(visc), None) == _lib.CB_ERR_UNSUPPORTED
+    assert "inviscid" in L.cb_last_error().decode()
+    assert L.cb_batch_set_variant(None, 2, 3, 0) == _lib.CB_ERR_ARG
+    assert L.cb_batch_run(None, 1) == _lib.CB_ERR_ARG
+    assert L.cb_batch_release(None, 0) == _lib.CB_ERR_ARG
+    assert L.cb_batch_info(None, 0, None, None) == _lib.CB_ERR_ARG
+    assert L.cb_batch_destroy(None) == _lib.CB_OK and L.cb_mesh_destroy(None) == _lib.CB_OK

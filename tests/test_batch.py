@@ -1,0 +1,182 @@
+"""Batched LSRK(5,4) over many independent instances (cb_batch_*), against the
+FP64 oracle run instance by instance, and the batching properties: a result
+does not depend on what else is in the batch, on when the instance was
+admitted, or on the group shape chosen by the tuner.
+
+Tolerances: FP64 batch vs oracle 1e-12 relative L2 per field; FP32 batch vs
+the FP64 oracle 1e-5; alone-vs-in-the-mix and variant 0-vs-1 bit-identical.
+"""
+import numpy as np
+import pytest
+
+from conftest import cuda_available
+from dg_cases import fourier_case, oracle_run, relerr_fields, vortex_case
+from canary_b200 import batch as B
+from canary_b200 import CanaryError, dg
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not cuda_available(), reason="needs a CUDA GPU")]
+
+
+def _cases():
+    """(mesh, Q, dt, nsteps) of a mixed set: 2-D vortices of several orders,
+    sizes and parameters, and warped 3-D Fourier cubes."""
+    out = []
+    for N, n, beta, xc, yc, steps in [(3, 4, 5.0, 5.0, 5.0, 9), (5, 3, 2.0, 4.0, 6.0, 6),
+                                      (8, 2, 3.5, 6.0, 3.0, 4), (4, 5, 1.5, 3.0, 7.0, 8),
+                                      (1, 6, 5.0, 5.0, 5.0, 5), (6, 3, 4.0, 5.5, 4.5, 7)]:
+        m, Q = vortex_case(N, n, beta, xc, yc)
+        out.append((m, Q, 0.002, steps))
+    # low orders take a fraction of the CFL step: the k <= 4 Fourier state is
+    # under-resolved there (the oracle itself blows up at the full step)
+    for N, n, steps, scale in [(3, 4, 5, 1.0), (7, 2, 3, 1.0), (2, 6, 6, 0.25), (1, 8, 5, 0.1)]:
+        m, Q, dt = fourier_case(N, n)
+        out.append((m, Q, dt * scale, steps))
+    return out
+
+
+@pytest.fixture(scope="module")
+def cases():
+    return _cases()
+
+
+@pytest.fixture(scope="module")
+def oracle_results(cases):
+    return [oracle_run(m, Q, dt, k) for (m, Q, dt, k) in cases]
+
+
+def _run_batch(cases, precision, idx=None, chunks=(2, 3, 100), variants=None):
+    """Admit cases[idx] into one batch, run in the given chunks, return the
+    final FP64 host states."""
+    idx = range(len(cases)) if idx is None else idx
+    b = B.Batch(precision, max_instances=64)
+    for (dim, N, v) in (variants or []):
+        b.set_variant(dim, N, v)
+    meshes, slots = [], []
+    for i in idx:
+        m, Q, dt, k = cases[i]
+        bm = B.BatchMesh(dg.DeviceMesh.upload(m), precision)
+        meshes.append(bm)
+        slots.append(b.add_state(bm, Q, dt, k))
+    for c in chunks:
+        b.run(c)
+    assert not b.status().any()
+    out = [b.result(s) for s in slots]
+    b.close()
+    return out
+
+
+def test_batch_fp64_matches_oracle(cases, oracle_results):
+    out = _run_batch(cases, 64)
+    for (m, Q, dt, k), ref, got in zip(cases, oracle_results, out):
+        err = max(relerr_fields(got, ref))
+        assert err < 1e-12, (m.dim, m.N, m.nelem, err)
+
+
+def test_batch_fp32_matches_oracle(cases, oracle_results):
+    out = _run_batch(cases, 32)
+    for (m, Q, dt, k), ref, got in zip(cases, oracle_results, out):
+        err = max(relerr_fields(got, ref))
+        assert err < 1e-5, (m.dim, m.N, m.nelem, err)
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_batch_result_same_alone_and_in_mix(cases, precision):
+    alone = [_run_batch(cases, precision, idx=[i], chunks=(100,))[0] for i in (0, 3, 7)]
+    mixed = _run_batch(cases, precision, chunks=(1, 1, 5, 100))
+    for a, i in zip(alone, (0, 3, 7)):
+        assert np.array_equal(a, mixed[i])
+
+
+def test_batch_variants_are_bit_identical(cases):
+    v0 = _run_batch(cases, 64)
+    var1 = [(2, N, 1) for N in (1, 3, 4, 5, 6, 8)] + [(3, N, 1) for N in (1, 2, 3)]
+    v1 = _run_batch(cases, 64, variants=var1)
+    for a, b in zip(v0, v1):
+        assert np.array_equal(a, b)
+
+
+def test_unbuilt_variant_is_rejected():
+    b = B.Batch(64, 4)
+    with pytest.raises(CanaryError):
+        b.set_variant(3, 7, 1)  # 3-D N=7 groups of 1024 nodes are not built
+    b.close()
+
+
+def test_continuous_batching_admit_and_release(cases):
+    """Instances admitted while others run, released as they finish, slots
+    reused and work lists compacted: each result equals the instance alone."""
+    alone = [_run_batch(cases, 64, idx=[i], chunks=(100,))[0] for i in range(len(cases))]
+    b = B.Batch(64, max_instances=3)
+    meshes = {}
+    pending = list(range(len(cases)))
+    live = {}
+    got = {}
+    rounds = 0
+    while pending or live:
+        # admit while slots are free
+        while pending and len(live) < 3:
+            i = pending.pop(0)
+            m, Q, dt, k = cases[i]
+            bm = meshes.setdefault(i, B.BatchMesh(dg.DeviceMesh.upload(m), 64))
+            live[b.add_state(bm, Q, dt, k)] = i
+        b.run(2)
+        rounds += 1
+        for s in list(live):
+            done, target = b.info(s)
+            if done == target:
+                got[live.pop(s)] = b.result(s)
+    b.close()
+    assert rounds > 3
+    for i in range(len(cases)):
+        assert np.array_equal(got[i], alone[i]), i
+
+
+def test_many_small_instances_force_list_growth_and_compaction():
+    """Hundreds of admissions and releases of small instances exercise work
+    list growth, in-place compaction and generation tags."""
+    m, Q = vortex_case(1, 40)  # N=1: 64 elements per group, 25 groups
+    ref = _run_batch([(m, Q, 0.002, 3)], 64, chunks=(100,))[0]
+    bm = B.BatchMesh(dg.DeviceMesh.upload(m), 64)
+    b = B.Batch(64, max_instances=48)
+    slots = [b.add_state(bm, Q, 0.002, 3) for _ in range(48)]
+    for cycle in range(4):
+        b.run(1)
+        # release every other slot, re-admit into the freed slots
+        for s in slots[cycle % 2::2]:
+            b.release(s)
+        for j in range(cycle % 2, 48, 2):
+            slots[j] = b.add_state(bm, Q, 0.002, 3)
+    b.run(10)
+    for s in slots:
+        assert np.array_equal(b.result(s), ref)
+    b.close()
+
+
+def test_nonfinite_state_flags_only_its_slot(cases):
+    m, Q, dt, k = cases[0]
+    bad = Q.copy(order="F")
+    bad[:, 2, 0] = -1.0  # negative density: the pressure's sqrt gives NaN
+    b = B.Batch(64, 8)
+    bm = B.BatchMesh(dg.DeviceMesh.upload(m), 64)
+    s_good = b.add_state(bm, Q, dt, k)
+    s_bad = b.add_state(bm, bad, dt, k)
+    b.run(k)
+    st = b.status()
+    assert st[s_bad] != 0 and st[s_good] == 0
+    good = b.result(s_good)
+    alone = _run_batch(cases, 64, idx=[0], chunks=(100,))[0]
+    assert np.array_equal(good, alone)
+    b.close()
+
+
+def test_batch_matches_single_solver(cases):
+    """Same instance through cb_lsrk_run (pipelined single-mesh kernel) and the
+    batch (grouped kernel): same arithmetic up to round-off."""
+    m, Q, dt, k = cases[7]  # 3-D N=7
+    s = dg.LSRK.for_state(dg.DeviceMesh.upload(m), Q, 64)
+    s.run(k, dt)
+    single = s.state()
+    s.close()
+    got = _run_batch(cases, 64, idx=[7], chunks=(100,))[0]
+    assert max(relerr_fields(got, single)) < 1e-13
