@@ -19,6 +19,12 @@ from ._lib import check
 from .dg import DeviceMesh, _ptr, _stream, _torch, from_device, make_phys, nstate, to_device
 
 MAX_ORDER = {2: 8, 3: 7}  # orders compiled into the batched stage
+# stage variants of one (dim, N): 0 = pipelined bulk-copy staging (where the
+# slabs are 16-byte multiples), 1 / 2 = grouped stage with ~256 / ~512 nodes
+# per block, 3 / 4 = pipelined staging compiled for 3 / 4 resident blocks per
+# SM (blocks of up to 256 threads)
+VARIANTS = (0, 1, 2, 3, 4)
+PIPELINED = (0, 3, 4)
 
 
 class BatchMesh:
@@ -67,8 +73,8 @@ class Batch:
         self._inst = {}  # slot -> (mesh, Q, rhs, offset)
 
     def set_variant(self, dim: int, N: int, variant: int) -> None:
-        """Group shape for instances of (dim, N) admitted from now on
-        (0: ~256 nodes per block, 1: ~512)."""
+        """Stage variant for instances of (dim, N) admitted from now on
+        (VARIANTS); raises CanaryError for a variant not built for it."""
         check(_lib.lib().cb_batch_set_variant(self._h, dim, N, variant))
 
     def add(self, mesh: BatchMesh, Q, rhs, dt: float, nsteps: int, qref=None) -> int:
@@ -229,8 +235,9 @@ class VortexEnsemble:
 # ------------------------------------------------------------------ autotuner
 def autotune(precision: int, shapes, nodes_target: int = 4_000_000, steps: int = 4, repeat: int = 3,
              stream=None) -> dict:
-    """Choose the element-group variant (elements per block) of each (dim, N)
-    by timing the batched step on a synthetic instance of that shape with
+    """Choose the stage variant (pipelined staging or grouped, and elements
+    per block) of each (dim, N) by timing the batched step on a synthetic
+    instance of that shape with
     about `nodes_target` nodes: 2-D vortex / 3-D free-stream-plus-Fourier
     states on periodic meshes.  Returns {(dim, N): variant}."""
     torch = _torch()
@@ -250,7 +257,7 @@ def autotune(precision: int, shapes, nodes_target: int = 4_000_000, steps: int =
             Q = np.stack(fourier_state(x, y, z, seed=0, device="cuda"), axis=1)
             dt = 1e-5
         timings = {}
-        for var in (0, 1):
+        for var in VARIANTS:
             b = Batch(precision, 1)
             try:
                 b.set_variant(dim, N, var)

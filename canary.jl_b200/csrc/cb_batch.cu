@@ -2,249 +2,77 @@
 // size: cb_mesh_* and cb_batch_* in include/canary_b200.h.
 //
 // Every admitted instance advances in one graph launch per LSRK step.  Each
-// group shape (dim, order N, variant) present has its own persistent kernel
-// that walks a device-resident work list of element groups (slot, first
-// element, generation) of that shape; the kernels of different shapes are
-// independent chains of the graph and run concurrently, and a small kernel at
-// the end of the step advances the per-slot step counters.  A group holds EPB
-// consecutive elements of one instance, EPB chosen so that a group carries
-// about 256 (variant 0) or 512 (variant 1) nodes; one kernel per shape keeps
-// each shape's registers and shared memory at what that shape needs.
+// group shape (dim, order N, stage variant) present has its own persistent
+// kernel that walks a device-resident work list of that shape; the kernels of
+// different shapes are independent chains of the graph and run concurrently,
+// and a one-thread kernel at the end of the step advances the batch step
+// counter.  A work item (16 bytes) names a group of consecutive elements of
+// one instance; the instance's pointers, dt, offsets and step window live in a
+// small per-slot descriptor table that stays in cache.  One kernel per shape
+// keeps each shape's registers and shared memory at what that shape needs;
+// the variants (pipelined bulk-copy staging at several occupancies, or
+// grouped staging with ~256 / ~512 nodes per block) are chosen per (dim, N)
+// by an autotuner and do not change the results.
 //
 // Membership is dynamic, for continuous batching: admitting an instance
-// launches one small kernel that writes its descriptor into the slot table and
-// appends its items to its shape's work list (no host staging buffer);
-// releasing it invalidates the slot, so stale items are skipped by their
-// generation tag, and a list is compacted when dead items dominate.  The
-// kernels read the lists through a device header, so admissions and releases
-// re-build the graph only when the set of shapes present changes.  Each
-// instance has its own dt and step target: its items are skipped once it has
-// taken all of its steps.  The state ping-pongs between the caller's buffer
-// and a batch-owned twin from a stream-ordered pool; the current buffer of an
-// instance at stage s of its step k is (k + s) mod 2.
+// launches one small kernel that writes its descriptor and appends its items
+// to its shape's list (no host staging buffer); releasing it invalidates its
+// items in place, and a list is compacted when invalid items dominate.  The kernels read the lists
+// through a device header, so admissions and releases re-build the graph only
+// when the set of shapes present changes.  Each instance has its own dt and
+// step count: its records are skipped once it has taken all of its steps.
+// The state ping-pongs between the caller's buffer and a batch-owned twin
+// from a stream-ordered pool; at batch step k the current buffer of an
+// instance admitted at step k0 is (k - k0 + stage) mod 2.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <bitset>
 #include <cmath>
 #include <cstring>
 #include <vector>
 
 #include "../../include/canary_b200.h"
-#include "cb_kernels.cuh"
+#include "cb_batch.cuh"
 #include "cb_ops.h"
 
 namespace cb {
 int solver_fail(int code, const char *fmt, ...);
 
-constexpr int BT = 256;                // threads per block of the batched stage
-constexpr int BMAXN2 = 8, BMAXN3 = 7;  // orders compiled into the batched stage
+// One batch step done: advance the batch step counter.
+__global__ void k_batch_step_end(BHdr *hdr) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) hdr->step += 1;
+}
 
-// Group shape for (dim, Nq, variant) at BT threads.
-template <int DIM, int Nq, int V>
-struct BCfg {
-  static constexpr int Np = ipow(Nq, DIM), Nfp = ipow(Nq, DIM - 1), NFACE = 2 * DIM;
-  static constexpr int BASE = Np >= BT ? 1 : BT / Np;
-  static constexpr int EPB = BASE * (V + 1);
-  static constexpr int SLOTS = EPB * Np;
-  static constexpr int NPT = cdiv(SLOTS, BT);
-  static constexpr int FSLOTS = EPB * NFACE * Nfp;
-  static constexpr int FPT = cdiv(FSLOTS, BT);
-  static constexpr bool OK = NPT <= 2;  // variants with more nodes per thread are not built
-};
-
+// Write the work items [pos, pos + ngroups) of the instance in `slot` into
+// list `sid` (groups of epb elements of nelem); when `d` is given, also its
+// descriptor, and reset its status word; set the list length to `count` when
+// count >= 0.
 template <typename T>
-struct BInst {
-  T *Q[2];  // Q[0]: the caller's state, Q[1]: the batch-owned twin
-  T *rhs;   // residual carry (caller's)
-  const T *vgeo, *sgeo, *D;
-  const int32_t *nbr;
-  int64_t nelem;
-  double dt;
-  int64_t done, target;  // steps taken / steps to take
-  int32_t N, var, gen, pad;
-  T qref[5];
-};
-struct BWork {
-  int32_t slot, e0, gen, pad;
-};
-// Shape id of (dim, N, variant); ids of orders that are not built stay unused.
-constexpr int NSHAPE = 2 * 2 * (BMAXN2 + 1);
-__host__ __device__ constexpr int shape_id(int dim, int N, int var) {
-  return (dim - 2) * 2 * (BMAXN2 + 1) + 2 * N + var;
-}
-struct BHdr {
-  BWork *work[NSHAPE];
-  int32_t nwork[NSHAPE];
-};
-
-// One group of the fused stage (volume + face + LSRK update) of one instance.
-template <int DIM, int Nq, int V, typename T>
-__device__ __forceinline__ void stage_group(const BInst<T> &I, int64_t e0, int par, const PhysT<T> &p, T rka,
-                                            T rkbdt, unsigned *ist, unsigned char *smem) {
-  using C = BCfg<DIM, Nq, V>;
-  constexpr int NS = Lay<DIM>::NS, NVG = Lay<DIM>::NVG, NSG = Lay<DIM>::NSG, IR = Lay<DIM>::IR;
-  constexpr int Np = C::Np, Nfp = C::Nfp, NF = C::NFACE, SP = C::SLOTS, FS = C::EPB * Nfp;
-  constexpr int MJI = DIM * DIM + 1, GC = DIM * DIM + 2 + DIM - 1;
-  const T *__restrict__ Qin = I.Q[par];
-  T *__restrict__ Qout = I.Q[par ^ 1];
-  T *__restrict__ rhs = I.rhs;
-  const T *__restrict__ vgeo = I.vgeo;
-  const int64_t nelem = I.nelem;
-  T *Ds = reinterpret_cast<T *>(smem);
-  T *sQ = Ds + ((Nq * Nq + 1) & ~1);  // [NS][SP]
-  T *sF = sQ + NS * SP;               // [DIM][NS][SP], reused as the face buffer
-  for (int t = threadIdx.x; t < Nq * Nq; t += BT) Ds[t] = I.D[t];
-  T R[C::NPT][NS];
-  // ---- pointwise contravariant fluxes
-#pragma unroll
-  for (int u = 0; u < C::NPT; ++u) {
-    const int slot = threadIdx.x + u * BT;
-    const int el = slot / Np, n = slot % Np;
-    const int64_t e = e0 + el;
-    if (slot < SP && e < nelem) {
-      T q[NS];
-#pragma unroll
-      for (int s = 0; s < NS; ++s) {
-        const T d = Qin[n + Np * (s + NS * e)];
-        sQ[s * SP + slot] = d;
-        q[s] = d + I.qref[s];
-        R[u][s] = rhs[n + Np * (s + NS * e)];
-      }
-      const T *vg = vgeo + (int64_t)Np * NVG * e;
-      T met[DIM][DIM], MJ;
-      load_metric<DIM, T>(vg, n, Np, met, MJ);
-      const T gc = p.grav != T(0) ? vg[n + Np * GC] : T(0);
-      const T ri = T(1) / q[IR];
-      const T P = pressure_ri<DIM, T>(q, ri, gc, p);
-      T f[NS][DIM];
-      euler_flux_ri<DIM, T>(q, ri, P, f);
-#pragma unroll
-      for (int r = 0; r < DIM; ++r)
-#pragma unroll
-        for (int s = 0; s < NS; ++s) {
-          T a = met[r][0] * f[s][0] + met[r][1] * f[s][1];
-          if (DIM == 3) a = a + met[r][2] * f[s][2];
-          sF[(r * NS + s) * SP + el * Np + n] = MJ * a;
-        }
-      R[u][DIM - 1] -= MJ * q[IR] * p.grav;
-    }
-  }
-  __syncthreads();
-  // ---- volume contraction
-#pragma unroll
-  for (int u = 0; u < C::NPT; ++u) {
-    const int slot = threadIdx.x + u * BT;
-    const int el = slot / Np, n = slot % Np;
-    if (slot < SP && e0 + el < nelem) contract<DIM, Nq, C::EPB, T>(sF, Ds, el, n, R[u]);
-  }
-  __syncthreads();
-  // ---- face fluxes into FF[NF][NS][EPB*Nfp] (aliases sF)
-  T *FF = sF;
-#pragma unroll
-  for (int u = 0; u < C::FPT; ++u) {
-    const int fs = threadIdx.x + u * BT;
-    if (fs >= C::FSLOTS) break;
-    const int el = fs / (NF * Nfp), f = (fs / Nfp) % NF, fn = fs % Nfp;
-    const int64_t e = e0 + el;
-    if (e >= nelem) continue;
-    const int vM = face_node<DIM, Nq>(f, fn);
-    const T *sg = I.sgeo + (int64_t)NSG * (fn + (int64_t)Nfp * (f + NF * e));
-    T nrm[DIM];
-#pragma unroll
-    for (int c = 0; c < DIM; ++c) nrm[c] = sg[c];
-    const T smj = sg[DIM];
-    T qM[NS], qP[NS];
-#pragma unroll
-    for (int s = 0; s < NS; ++s) qM[s] = sQ[s * SP + el * Np + vM] + I.qref[s];
-    const T gM = p.grav != T(0) ? vgeo[vM + Np * (GC + NVG * e)] : T(0);
-    const T riM = T(1) / qM[IR];
-    const T PM = pressure_ri<DIM, T>(qM, riM, gM, p);
-    const int32_t nb = I.nbr[f + NF * e];
-    T PP, riP;
-    if (nb >= 0) {
-      const int64_t e2 = nb >> 3;
-      const int vP = face_node<DIM, Nq>(nb & 7, fn);
-#pragma unroll
-      for (int s = 0; s < NS; ++s) qP[s] = Qin[vP + Np * (s + NS * e2)] + I.qref[s];
-      const T gP = p.grav != T(0) ? vgeo[vP + Np * (GC + NVG * e2)] : T(0);
-      riP = T(1) / qP[IR];
-      PP = pressure_ri<DIM, T>(qP, riP, gP, p);
-    } else {
-      wall_state<DIM, T>(qM, nrm, qP);
-      riP = riM;
-      PP = PM;
-    }
-    T out[NS];
-    rusanov_n<DIM, T>(qM, riM, PM, qP, riP, PP, nrm, p, out);
-#pragma unroll
-    for (int s = 0; s < NS; ++s) FF[(f * NS + s) * FS + el * Nfp + fn] = smj * out[s];
-  }
-  __syncthreads();
-  // ---- face accumulation and LSRK update
-  bool bad = false;
-#pragma unroll
-  for (int u = 0; u < C::NPT; ++u) {
-    const int slot = threadIdx.x + u * BT;
-    const int el = slot / Np, n = slot % Np;
-    const int64_t e = e0 + el;
-    if (slot < SP && e < nelem) {
-      gather_face_terms<DIM, Nq, C::EPB, T>(FF, el, n, R[u]);
-      const T mji = vgeo[n + Np * (MJI + (int64_t)NVG * e)];
-#pragma unroll
-      for (int s = 0; s < NS; ++s) {
-        const T qn = sQ[s * SP + slot] + rkbdt * R[u][s] * mji;
-        bad |= !isfinite(qn);
-        Qout[n + Np * (s + NS * e)] = qn;
-        rhs[n + Np * (s + NS * e)] = R[u][s] * rka;
-      }
-    }
-  }
-  if (bad) atomicOr(ist, ST_NONFINITE);
-  __syncthreads();  // shared memory is reused by the block's next item
-}
-
-// Persistent stage kernel of one group shape: the blocks stride over the
-// shape's work list.
-template <int DIM, int Nq, int V, typename T>
-__global__ void __launch_bounds__(BT, 2)
-k_stage_batch(const BInst<T> *__restrict__ insts, const BHdr *__restrict__ hdr, int stage, PhysT<T> p, T rka,
-              double rkb, unsigned *__restrict__ status) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  constexpr int SID = shape_id(DIM, Nq - 1, V);
-  const int nwork = hdr->nwork[SID];
-  const BWork *__restrict__ work = hdr->work[SID];
-  for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
-    const BWork it = work[w];
-    const BInst<T> &I = insts[it.slot];
-    if (I.gen != it.gen || I.done >= I.target) continue;  // uniform over the block
-    const int par = (int)((I.done + stage) & 1);
-    stage_group<DIM, Nq, V, T>(I, it.e0, par, p, rka, T(rkb * I.dt), status + it.slot, smem_raw);
-  }
-}
-
-// Advance the step counter of every slot that still has steps to take.
-template <typename T>
-__global__ void k_batch_step_end(BInst<T> *insts, int cap) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < cap && insts[i].done < insts[i].target) insts[i].done += 1;
-}
-
-// Write a slot descriptor (when `write`) and the work items [pos, pos+ngroups)
-// of that slot into list `sid`; set the list length to pos+ngroups when
-// `set_count`.
-template <typename T>
-__global__ void k_batch_admit(BInst<T> *insts, int slot, BInst<T> val, int write, unsigned *status, BHdr *hdr,
-                              int sid, int pos, int ngroups, int epb, int set_count) {
+__global__ void k_batch_admit(BHdr *hdr, int sid, int slot, BDesc<T> d, int write, int pos, int ngroups, int epb,
+                              int64_t nelem, int count) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t == 0) {
     if (write) {
-      insts[slot] = val;
-      status[slot] = 0;
+      static_cast<BDesc<T> *>(hdr->desc)[slot] = d;
+      *d.status = 0;
     }
-    if (set_count) hdr->nwork[sid] = pos + ngroups;
+    if (count >= 0) hdr->nwork[sid] = count;
   }
   BWork *work = hdr->work[sid];
-  for (int g = t; g < ngroups; g += gridDim.x * blockDim.x) work[pos + g] = BWork{slot, g * epb, val.gen, 0};
+  for (int g = t; g < ngroups; g += gridDim.x * blockDim.x) {
+    const int64_t e0 = (int64_t)g * epb, rem = nelem - e0;
+    work[pos + g] = BWork{slot, (int32_t)e0, rem < epb ? (int32_t)rem : epb, 1};
+  }
+}
+
+// Invalidate the work items [pos, pos + n) of list `sid` and set its length
+// to `count`.
+__global__ void k_batch_invalidate(BHdr *hdr, int sid, int pos, int n, int count) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t == 0) hdr->nwork[sid] = count;
+  BWork *work = hdr->work[sid];
+  for (int g = t; g < n; g += gridDim.x * blockDim.x) work[pos + g].valid = 0;
 }
 
 __global__ void k_batch_hdr(BHdr *hdr, int sid, BWork *ptr, int nwork) {
@@ -254,67 +82,41 @@ __global__ void k_batch_hdr(BHdr *hdr, int sid, BWork *ptr, int nwork) {
   }
 }
 
-inline int b_base(int dim, int N) {
-  const int Nq = N + 1, Np = dim == 2 ? Nq * Nq : Nq * Nq * Nq;
-  return Np >= BT ? 1 : BT / Np;
-}
-inline bool b_order_ok(int dim, int N) { return N >= 1 && N <= (dim == 2 ? BMAXN2 : BMAXN3); }
-inline bool b_var_ok(int dim, int N, int var) {
-  if (!b_order_ok(dim, N) || (var != 0 && var != 1)) return false;
-  if (var == 0) return true;
-  const int Nq = N + 1, Np = dim == 2 ? Nq * Nq : Nq * Nq * Nq;
-  return (2 * b_base(dim, N) * Np + BT - 1) / BT <= 2;
-}
-template <typename T>
-size_t b_smem(int dim, int N, int var) {
-  const int Nq = N + 1, Np = dim == 2 ? Nq * Nq : Nq * Nq * Nq, NS = dim == 2 ? 4 : 5;
-  const size_t slots = (size_t)b_base(dim, N) * (var + 1) * Np;
-  return sizeof(T) * (((Nq * Nq + 1) & ~1) + NS * slots + (size_t)dim * NS * slots);
-}
-
-// Host table of the stage kernels, indexed by shape id.
-template <typename T>
-struct BKernels {
-  const void *fn[NSHAPE] = {};
-  int grid[NSHAPE] = {};
-  bool ready[NSHAPE] = {};
-};
-template <int DIM, int Nq, typename T>
-void b_fill(BKernels<T> &k) {
-  k.fn[shape_id(DIM, Nq - 1, 0)] = (const void *)k_stage_batch<DIM, Nq, 0, T>;
-  if (BCfg<DIM, Nq, 1>::OK)
-    k.fn[shape_id(DIM, Nq - 1, 1)] = (const void *)k_stage_batch<DIM, Nq, BCfg<DIM, Nq, 1>::OK ? 1 : 0, T>;
-}
 template <typename T>
 BKernels<T> &b_kernels() {
   static BKernels<T> k = [] {
     BKernels<T> t;
-    b_fill<2, 2, T>(t); b_fill<2, 3, T>(t); b_fill<2, 4, T>(t); b_fill<2, 5, T>(t);
-    b_fill<2, 6, T>(t); b_fill<2, 7, T>(t); b_fill<2, 8, T>(t); b_fill<2, 9, T>(t);
-    b_fill<3, 2, T>(t); b_fill<3, 3, T>(t); b_fill<3, 4, T>(t); b_fill<3, 5, T>(t);
-    b_fill<3, 6, T>(t); b_fill<3, 7, T>(t); b_fill<3, 8, T>(t);
+    b_fill_dim<2, T>(t);
+    b_fill_dim<3, T>(t);
     return t;
   }();
   return k;
+}
+template <typename T>
+bool b_var_ok(int dim, int N, int var) {
+  return b_order_ok(dim, N) && var >= 0 && var < NVAR && b_kernels<T>().fn[shape_id(dim, N, var)] != nullptr;
+}
+// default variant: the pipelined stage where it is built, else 512-node groups
+// (the autotuner may choose another)
+template <typename T>
+int b_default_var(int dim, int N) {
+  return b_var_ok<T>(dim, N, 0) ? 0 : b_var_ok<T>(dim, N, 2) ? 2 : 1;
 }
 // Shared-memory limit and persistent grid (all SMs at the occupancy that the
 // shape's registers and shared memory allow) of one shape, set up once per
 // process on the current device.
 template <typename T>
-cudaError_t b_prepare(int dim, int N, int var, const void **fn, size_t *smem, int *grid) {
+cudaError_t b_prepare(int sid) {
   BKernels<T> &k = b_kernels<T>();
-  const int sid = shape_id(dim, N, var);
-  *fn = k.fn[sid];
-  *smem = b_smem<T>(dim, N, var);
   if (!k.ready[sid]) {
-    cudaError_t e = cudaFuncSetAttribute(k.fn[sid], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem);
+    cudaError_t e = cudaFuncSetAttribute(k.fn[sid], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem[sid]);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.fn[sid], BT, *smem)) != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.fn[sid], k.threads[sid], k.smem[sid]);
+    if (e != cudaSuccess) return e;
     k.grid[sid] = num_sms() * std::max(per_sm, 1);
     k.ready[sid] = true;
   }
-  *grid = k.grid[sid];
   return cudaSuccess;
 }
 
@@ -340,11 +142,13 @@ const double RKB[5] = {1432997174477.0 / 9575080441755.0, 5161836677717.0 / 1361
 
 struct BSlot {
   bool used = false;
-  int dim = 0, N = 0, var = 0, sid = 0, epb = 1, gen = 0;
+  int dim = 0, N = 0, var = 0, sid = 0, epb = 1;
   int64_t nelem = 0, start = 0, target = 0;
   int pos = 0, ngroups = 0;
   size_t qbytes = 0;
   void *Q = nullptr, *alt = nullptr;
+  BDesc<double> d64{};  // template record of the instance (the batch's precision)
+  BDesc<float> d32{};
 };
 
 // Work list of one shape.
@@ -361,17 +165,16 @@ struct cb_batch {
   bool own_stream = false;
   cudaMemPool_t pool = nullptr;  // stream-ordered pool of state twins and work lists
   cb_phys phys{};
-  void *insts = nullptr;  // BInst<T>[cap]
-  unsigned *status = nullptr;
+  unsigned *status = nullptr;  // per slot
+  void *desc = nullptr;        // BDesc<T> per slot
   BHdr *hdr = nullptr;
   BList list[NSHAPE];
-  int nslots[NSHAPE] = {};  // live instances per shape
   std::vector<BSlot> slots;
-  int64_t steps = 0;
+  int64_t steps = 0;  // batch steps launched (the device counter after them)
   int var[2][BMAXN2 + 1] = {};
   // one step as a graph; re-built when the set of shapes present changes
   cudaGraphExec_t exec = nullptr;
-  uint64_t g_shapes = 0;
+  std::bitset<NSHAPE> g_shapes;
 };
 
 namespace {
@@ -379,15 +182,21 @@ namespace {
 void drop_graph(cb_batch *b) {
   if (b->exec) cudaGraphExecDestroy(b->exec);
   b->exec = nullptr;
-  b->g_shapes = 0;
+  b->g_shapes.reset();
 }
 
 template <typename T>
-cudaError_t launch_admit(cb_batch *b, int slot, const BInst<T> &val, bool write, int sid, int pos, int ngroups,
-                         int epb, bool set_count) {
-  const int blocks = std::max(1, std::min(1024, (ngroups + 255) / 256));
-  k_batch_admit<T><<<blocks, 256, 0, b->stream>>>((BInst<T> *)b->insts, slot, val, write ? 1 : 0, b->status,
-                                                  b->hdr, sid, pos, ngroups, epb, set_count ? 1 : 0);
+BDesc<T> &record(BSlot &s);
+template <>
+BDesc<double> &record<double>(BSlot &s) { return s.d64; }
+template <>
+BDesc<float> &record<float>(BSlot &s) { return s.d32; }
+
+template <typename T>
+cudaError_t launch_admit(cb_batch *b, int slot, const BSlot &sl, int pos, int count, bool write) {
+  const int blocks = std::max(1, std::min(1024, (sl.ngroups + 255) / 256));
+  k_batch_admit<T><<<blocks, 256, 0, b->stream>>>(b->hdr, sl.sid, slot, record<T>(const_cast<BSlot &>(sl)),
+                                                  write ? 1 : 0, pos, sl.ngroups, sl.epb, sl.nelem, count);
   return cudaGetLastError();
 }
 
@@ -401,12 +210,10 @@ cudaError_t compact(cb_batch *b, int sid, BWork *dst) {
     if (e != cudaSuccess) return e;
   }
   int pos = 0;
-  BInst<T> none{};
   for (int s = 0; s < b->cap; ++s) {
     BSlot &sl = b->slots[s];
     if (!sl.used || sl.sid != sid) continue;
-    none.gen = sl.gen;
-    cudaError_t e = launch_admit<T>(b, s, none, false, sid, pos, sl.ngroups, sl.epb, false);
+    cudaError_t e = launch_admit<T>(b, s, sl, pos, -1, false);
     if (e != cudaSuccess) return e;
     sl.pos = pos;
     pos += sl.ngroups;
@@ -416,16 +223,16 @@ cudaError_t compact(cb_batch *b, int sid, BWork *dst) {
   return cudaGetLastError();
 }
 
-// Make room for `need` more items in list `sid`: compact in place when the
-// live items then fill at most three quarters of it, else move to a larger
+// Make room for `need` more records in list `sid`: compact in place when the
+// live records then fill at most three quarters of it, else move to a larger
 // list.
 template <typename T>
 cudaError_t ensure_work(cb_batch *b, int sid, int need) {
   BList &L = b->list[sid];
   if ((int64_t)L.tail + need <= L.cap) return cudaSuccess;
   if (((int64_t)L.live + need) * 4 <= (int64_t)L.cap * 3) return compact<T>(b, sid, nullptr);
-  const int64_t ncap = std::max<int64_t>({(int64_t)L.cap * 2, ((int64_t)L.live + need) * 2, 1024});
-  if (ncap > (1ll << 30)) return cudaErrorMemoryAllocation;
+  const int64_t ncap = std::max<int64_t>({(int64_t)L.cap * 2, ((int64_t)L.live + need) * 2, 256});
+  if (ncap > (1ll << 28)) return cudaErrorMemoryAllocation;
   BWork *nw = nullptr;
   cudaError_t e = cudaMallocFromPoolAsync((void **)&nw, sizeof(BWork) * ncap, b->pool, b->stream);
   if (e != cudaSuccess) return e;
@@ -440,37 +247,37 @@ cudaError_t ensure_work(cb_batch *b, int sid, int need) {
 // kernels (the chains are independent and run concurrently), then the step
 // counter kernel after all chains.
 template <typename T>
-cudaError_t build_graph(cb_batch *b, uint64_t shapes) {
+cudaError_t build_graph(cb_batch *b, const std::bitset<NSHAPE> &shapes) {
   const PhysT<T> p(Phys{b->phys.gamma, b->phys.R_gas, b->phys.c_p, b->phys.c_v, b->phys.gravity, b->phys.Pr,
                         b->phys.lambda, b->phys.visc});
   cudaGraph_t g = nullptr;
   cudaError_t e = cudaGraphCreate(&g, 0);
   if (e != cudaSuccess) return e;
   std::vector<cudaGraphNode_t> lasts;
-  const BInst<T> *insts = (const BInst<T> *)b->insts;
   const BHdr *hdr = b->hdr;
-  unsigned *status = b->status;
+  const BKernels<T> &K = b_kernels<T>();
+  // the pipelined kernels of every (dim, N) take a BatchSrc whose layout does
+  // not depend on its template arguments
+  using SrcArgs = BatchSrc<T, 5, 1>;
+  static_assert(sizeof(SrcArgs) == sizeof(BatchSrc<T, 4, 64>), "BatchSrc layout");
   for (int sid = 0; sid < NSHAPE && e == cudaSuccess; ++sid) {
-    if (!(shapes >> sid & 1)) continue;
-    const int dim = 2 + sid / (2 * (BMAXN2 + 1)), N = (sid % (2 * (BMAXN2 + 1))) / 2, var = sid % 2;
-    const void *fn;
-    size_t smem;
-    int grid;
-    if ((e = b_prepare<T>(dim, N, var, &fn, &smem, &grid)) != cudaSuccess) break;
+    if (!shapes.test(sid)) continue;
+    if ((e = b_prepare<T>(sid)) != cudaSuccess) break;
     cudaGraphNode_t prev = nullptr;
     for (int st = 0; st < 5 && e == cudaSuccess; ++st) {
       int stage = st;
       T rka = T(RKA[(st + 1) % 5]);
       double rkb = RKB[st];
       PhysT<T> pp = p;
-      void *args[] = {(void *)&insts, (void *)&hdr, (void *)&stage, (void *)&pp, (void *)&rka, (void *)&rkb,
-                      (void *)&status};
+      SrcArgs src{hdr, sid, st, rkb, nullptr, nullptr, -1};
+      void *gargs[] = {(void *)&hdr, (void *)&stage, (void *)&pp, (void *)&rka, (void *)&rkb};
+      void *pargs[] = {(void *)&src, (void *)&pp, (void *)&rka};
       cudaKernelNodeParams kp{};
-      kp.func = (void *)fn;
-      kp.gridDim = dim3(grid);
-      kp.blockDim = dim3(BT);
-      kp.sharedMemBytes = (unsigned)smem;
-      kp.kernelParams = args;
+      kp.func = (void *)K.fn[sid];
+      kp.gridDim = dim3(K.grid[sid]);
+      kp.blockDim = dim3(K.threads[sid]);
+      kp.sharedMemBytes = (unsigned)K.smem[sid];
+      kp.kernelParams = K.pipelined[sid] ? pargs : gargs;
       cudaGraphNode_t node;
       e = cudaGraphAddKernelNode(&node, g, prev ? &prev : nullptr, prev ? 1 : 0, &kp);
       prev = node;
@@ -478,13 +285,12 @@ cudaError_t build_graph(cb_batch *b, uint64_t shapes) {
     if (e == cudaSuccess) lasts.push_back(prev);
   }
   if (e == cudaSuccess) {
-    BInst<T> *mi = (BInst<T> *)b->insts;
-    int cap = b->cap;
-    void *args[] = {(void *)&mi, (void *)&cap};
+    BHdr *mh = b->hdr;
+    void *args[] = {(void *)&mh};
     cudaKernelNodeParams kp{};
-    kp.func = (void *)k_batch_step_end<T>;
-    kp.gridDim = dim3((b->cap + 255) / 256);
-    kp.blockDim = dim3(256);
+    kp.func = (void *)k_batch_step_end;
+    kp.gridDim = dim3(1);
+    kp.blockDim = dim3(32);
     kp.kernelParams = args;
     cudaGraphNode_t node;
     e = cudaGraphAddKernelNode(&node, g, lasts.data(), lasts.size(), &kp);
@@ -498,28 +304,27 @@ cudaError_t build_graph(cb_batch *b, uint64_t shapes) {
 template <typename T>
 int batch_run(cb_batch *b, int64_t nsteps) {
   int64_t need = 0;  // steps that some live instance still has to take
-  uint64_t shapes = 0;
+  std::bitset<NSHAPE> shapes;
   for (const BSlot &s : b->slots)
     if (s.used && s.start + s.target > b->steps) {
       need = std::max<int64_t>(need, s.start + s.target - b->steps);
-      shapes |= 1ull << s.sid;
+      shapes.set(s.sid);
     }
   const int64_t launch = std::min(need, nsteps);
-  if (launch > 0) {
-    if (!b->exec || shapes != b->g_shapes) {
+  if (launch <= 0) return CB_OK;
+  if (!b->exec || shapes != b->g_shapes) {
+    drop_graph(b);
+    cudaError_t e = build_graph<T>(b, shapes);
+    if (e != cudaSuccess) {
       drop_graph(b);
-      cudaError_t e = build_graph<T>(b, shapes);
-      if (e != cudaSuccess) {
-        drop_graph(b);
-        return solver_fail(CB_ERR_CUDA, "cb_batch_run: step graph: %s", cudaGetErrorString(e));
-      }
-    }
-    for (int64_t r = 0; r < launch; ++r) {
-      cudaError_t e = cudaGraphLaunch(b->exec, b->stream);
-      if (e != cudaSuccess) return solver_fail(CB_ERR_CUDA, "cb_batch_run: graph launch: %s", cudaGetErrorString(e));
+      return solver_fail(CB_ERR_CUDA, "cb_batch_run: step graph: %s", cudaGetErrorString(e));
     }
   }
-  b->steps += nsteps;
+  for (int64_t r = 0; r < launch; ++r) {
+    cudaError_t e = cudaGraphLaunch(b->exec, b->stream);
+    if (e != cudaSuccess) return solver_fail(CB_ERR_CUDA, "cb_batch_run: graph launch: %s", cudaGetErrorString(e));
+    ++b->steps;
+  }
   return CB_OK;
 }
 
@@ -535,10 +340,9 @@ int batch_add(cb_batch *b, const cb_mesh *m, void *Q, void *rhs, double dt, int6
   if (slot < 0) return solver_fail(CB_ERR_NOMEM, "cb_batch_add: all %d slots are in use", b->cap);
   const int Nq = m->N + 1, ns = m->dim == 2 ? 4 : 5;
   const int64_t Np = m->dim == 2 ? (int64_t)Nq * Nq : (int64_t)Nq * Nq * Nq;
-  BSlot &sl = b->slots[slot];
   const int var = b->var[m->dim - 2][m->N];
   const int sid = shape_id(m->dim, m->N, var);
-  const int epb = b_base(m->dim, m->N) * (var + 1);
+  const int epb = b_kernels<T>().epb[sid];
   const int64_t ngroups = (m->nelem + epb - 1) / epb;
   const size_t qbytes = sizeof(T) * Np * ns * m->nelem;
   void *alt = nullptr;
@@ -548,45 +352,42 @@ int batch_add(cb_batch *b, const cb_mesh *m, void *Q, void *rhs, double dt, int6
     cudaFreeAsync(alt, b->stream);
     return solver_fail(CB_ERR_NOMEM, "cb_batch_add: work list: %s", cudaGetErrorString(e));
   }
-  BInst<T> v{};
-  v.Q[0] = (T *)Q;
-  v.Q[1] = (T *)alt;
-  v.rhs = (T *)rhs;
-  v.vgeo = (const T *)m->vgeo;
-  v.sgeo = (const T *)m->sgeo;
-  v.D = (const T *)m->D;
-  v.nbr = m->nbr;
-  v.nelem = m->nelem;
-  v.dt = dt;
-  v.done = 0;
-  v.target = nsteps;
-  v.N = m->N;
-  v.var = var;
-  v.gen = sl.gen + 1;
-  for (int k = 0; k < 5; ++k) v.qref[k] = qref ? T(qref[k]) : T(0);
-  BList &L = b->list[sid];
-  const int pos = L.tail;
-  if ((e = launch_admit<T>(b, slot, v, true, sid, pos, (int)ngroups, epb, true)) != cudaSuccess) {
-    cudaFreeAsync(alt, b->stream);
-    return solver_fail(CB_ERR_CUDA, "cb_batch_add: %s", cudaGetErrorString(e));
-  }
+  BSlot sl;
   sl.used = true;
   sl.dim = m->dim;
   sl.N = m->N;
   sl.var = var;
   sl.sid = sid;
   sl.epb = epb;
-  sl.gen = v.gen;
   sl.nelem = m->nelem;
   sl.start = b->steps;
   sl.target = nsteps;
-  sl.pos = pos;
   sl.ngroups = (int)ngroups;
   sl.qbytes = qbytes;
   sl.Q = Q;
   sl.alt = alt;
-  L.tail = pos + (int)ngroups;
-  L.live += (int)ngroups;
+  BDesc<T> &d = record<T>(sl);
+  d.Q[0] = (T *)Q;
+  d.Q[1] = (T *)alt;
+  d.rhs = (T *)rhs;
+  d.vgeo = (const T *)m->vgeo;
+  d.sgeo = (const T *)m->sgeo;
+  d.D = (const T *)m->D;
+  d.nbr = m->nbr;
+  d.status = b->status + slot;
+  d.start = b->steps;
+  d.target = nsteps;
+  d.dt = dt;
+  for (int k = 0; k < 5; ++k) d.qref[k] = qref ? T(qref[k]) : T(0);
+  BList &L = b->list[sid];
+  sl.pos = L.tail;
+  if ((e = launch_admit<T>(b, slot, sl, sl.pos, sl.pos + sl.ngroups, true)) != cudaSuccess) {
+    cudaFreeAsync(alt, b->stream);
+    return solver_fail(CB_ERR_CUDA, "cb_batch_add: %s", cudaGetErrorString(e));
+  }
+  L.tail = sl.pos + sl.ngroups;
+  L.live += sl.ngroups;
+  b->slots[slot] = sl;
   *slot_out = slot;
   return CB_OK;
 }
@@ -599,17 +400,15 @@ int batch_release(cb_batch *b, int slot) {
   cudaError_t e = cudaSuccess;
   if (done & 1) e = cudaMemcpyAsync(sl.Q, sl.alt, sl.qbytes, cudaMemcpyDeviceToDevice, b->stream);
   if (e != cudaSuccess) return solver_fail(CB_ERR_CUDA, "cb_batch_release: copy: %s", cudaGetErrorString(e));
-  BInst<T> none{};
-  none.gen = sl.gen;  // target 0: the slot's items are skipped until the slot is reused
   L.live -= sl.ngroups;
   const int ntail = L.live == 0 ? 0 : sl.pos + sl.ngroups == L.tail ? sl.pos : L.tail;
-  if ((e = launch_admit<T>(b, slot, none, true, sl.sid, ntail, 0, 1, true)) != cudaSuccess)
+  const int blocks = std::max(1, std::min(1024, (sl.ngroups + 255) / 256));
+  k_batch_invalidate<<<blocks, 256, 0, b->stream>>>(b->hdr, sl.sid, sl.pos, sl.ngroups, ntail);
+  if ((e = cudaGetLastError()) != cudaSuccess)
     return solver_fail(CB_ERR_CUDA, "cb_batch_release: %s", cudaGetErrorString(e));
   L.tail = ntail;
   cudaFreeAsync(sl.alt, b->stream);
-  const int gen = sl.gen;
   sl = BSlot{};
-  sl.gen = gen;
   return CB_OK;
 }
 
@@ -703,6 +502,9 @@ int cb_batch_create(cb_batch **out, int precision, int max_instances, const cb_p
   b->cap = max_instances;
   b->phys = *phys;
   b->slots.resize(max_instances);
+  for (int dim = 2; dim <= 3; ++dim)
+    for (int N = 1; b_order_ok(dim, N); ++N)
+      b->var[dim - 2][N] = precision == 64 ? b_default_var<double>(dim, N) : b_default_var<float>(dim, N);
   cudaGetDevice(&b->device);
   cudaError_t e = cudaSuccess;
   auto bail = [&](const char *what) {
@@ -726,14 +528,17 @@ int cb_batch_create(cb_batch **out, int precision, int max_instances, const cb_p
     if ((e = cudaMemPoolSetAttribute(b->pool, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess)
       return bail("memory pool");
   }
-  const size_t ib = precision == 64 ? sizeof(BInst<double>) : sizeof(BInst<float>);
-  if ((e = cudaMalloc(&b->insts, ib * max_instances)) != cudaSuccess ||
-      (e = cudaMalloc((void **)&b->status, sizeof(unsigned) * max_instances)) != cudaSuccess ||
-      (e = cudaMalloc((void **)&b->hdr, sizeof(BHdr))) != cudaSuccess)
+  const size_t db = precision == 64 ? sizeof(BDesc<double>) : sizeof(BDesc<float>);
+  if ((e = cudaMalloc((void **)&b->status, sizeof(unsigned) * max_instances)) != cudaSuccess ||
+      (e = cudaMalloc((void **)&b->hdr, sizeof(BHdr))) != cudaSuccess ||
+      (e = cudaMalloc(&b->desc, db * max_instances)) != cudaSuccess)
     return bail("tables");
-  if ((e = cudaMemsetAsync(b->insts, 0, ib * max_instances, b->stream)) != cudaSuccess ||
-      (e = cudaMemsetAsync(b->status, 0, sizeof(unsigned) * max_instances, b->stream)) != cudaSuccess ||
-      (e = cudaMemsetAsync(b->hdr, 0, sizeof(BHdr), b->stream)) != cudaSuccess)
+  BHdr h0{};
+  h0.desc = b->desc;
+  if ((e = cudaMemsetAsync(b->status, 0, sizeof(unsigned) * max_instances, b->stream)) != cudaSuccess ||
+      (e = cudaMemsetAsync(b->desc, 0, db * max_instances, b->stream)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(b->hdr, &h0, sizeof h0, cudaMemcpyHostToDevice, b->stream)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(b->stream)) != cudaSuccess)
     return bail("tables");
   *out = b;
   return CB_OK;
@@ -742,7 +547,7 @@ int cb_batch_create(cb_batch **out, int precision, int max_instances, const cb_p
 int cb_batch_set_variant(cb_batch *b, int dim, int N, int variant) {
   if (!b || (dim != 2 && dim != 3) || !b_order_ok(dim, N))
     return solver_fail(CB_ERR_ARG, "cb_batch_set_variant: bad arguments");
-  if (!b_var_ok(dim, N, variant))
+  if (!(b->prec == 64 ? b_var_ok<double>(dim, N, variant) : b_var_ok<float>(dim, N, variant)))
     return solver_fail(CB_ERR_UNSUPPORTED, "cb_batch_set_variant: variant %d is not built for dim %d N %d",
                        variant, dim, N);
   b->var[dim - 2][N] = variant;
@@ -797,8 +602,8 @@ int cb_batch_destroy(cb_batch *b) {
   for (BList &L : b->list)
     if (L.buf) cudaFreeAsync(L.buf, b->stream);
   if (b->stream) cudaStreamSynchronize(b->stream);
-  cudaFree(b->insts);
   cudaFree(b->status);
+  cudaFree(b->desc);
   cudaFree(b->hdr);
   if (b->pool) cudaMemPoolDestroy(b->pool);
   if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);

@@ -1,0 +1,386 @@
+// Kernels and device-side types of the batched LSRK driver (cb_batch.cu).
+// The stage kernels of each (dim, precision) are instantiated in their own
+// translation unit (cb_batch_<dim>d_<prec>.cu) through b_fill_dim.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+
+#include "cb_kernels.cuh"
+
+namespace cb {
+
+constexpr int BT = 256;                // threads per block of the grouped stage
+constexpr int BMAXN2 = 8, BMAXN3 = 7;  // orders compiled into the batched stage
+
+// Shape of the grouped (non-pipelined) stage for (dim, Nq) at BT threads:
+// groups of about 256 (G = 0) or 512 (G = 1) nodes.
+template <int DIM, int Nq, int G>
+struct BCfg {
+  static constexpr int Np = ipow(Nq, DIM), Nfp = ipow(Nq, DIM - 1), NFACE = 2 * DIM;
+  static constexpr int BASE = Np >= BT ? 1 : BT / Np;
+  static constexpr int EPB = BASE * (G + 1);
+  static constexpr int SLOTS = EPB * Np;
+  static constexpr int NPT = cdiv(SLOTS, BT);
+  static constexpr int FSLOTS = EPB * NFACE * Nfp;
+  static constexpr int FPT = cdiv(FSLOTS, BT);
+  static constexpr bool OK = NPT <= 2;  // variants with more nodes per thread are not built
+};
+
+// Descriptor of one admitted instance (one per slot; the table is small and
+// stays in cache).  At batch step k the instance has taken k - start steps; it
+// is advanced while that is below `target`, and its current state is
+// Q[(k - start + stage) mod 2] at stage `stage`.
+template <typename T>
+struct alignas(16) BDesc {
+  T *Q[2];  // Q[0]: the caller's state, Q[1]: the batch-owned twin
+  T *rhs;   // residual carry (caller's)
+  const T *vgeo, *sgeo, *D;
+  const int32_t *nbr;
+  unsigned *status;  // the instance's status word
+  int64_t start, target;
+  double dt;
+  T qref[5];
+};
+// One work item: a group of `nv` consecutive elements (from e0) of the
+// instance in `slot`; written when the instance is admitted and invalidated
+// (valid = 0) when it is released.
+struct alignas(16) BWork {
+  int32_t slot, e0, nv, valid;
+};
+
+// Stage variants of one (dim, N): 0 = the pipelined bulk-copy stage
+// (k_stage_pipe2, groups of Cfg::EPB elements, state/metric/carry/face
+// geometry staged one group ahead) at its default occupancy (Pipe2::MINB
+// resident blocks per SM), 1 and 2 = the grouped stage with groups of about
+// 256 and 512 nodes, 3 and 4 = the pipelined stage compiled for the two other
+// occupancies among 2, 3 and 4 blocks per SM (blocks of up to 256 threads).
+// Shape id of (dim, N, variant); ids of shapes that are not built stay
+// unused.
+constexpr int NVAR = 5;
+constexpr int NSHAPE = 2 * NVAR * (BMAXN2 + 1);
+__host__ __device__ constexpr int shape_id(int dim, int N, int var) {
+  return (dim - 2) * NVAR * (BMAXN2 + 1) + NVAR * N + var;
+}
+// Device header: the instance table (BDesc<T>[slots]), the work list of
+// every shape and the batch step counter.
+struct BHdr {
+  void *desc;
+  BWork *work[NSHAPE];
+  int32_t nwork[NSHAPE];
+  int64_t step;
+};
+
+// One group of the fused stage (volume + face + LSRK update) of one instance.
+template <int DIM, int Nq, int G, typename T>
+__device__ __forceinline__ void stage_group(const BDesc<T> &I, int64_t e0, int nv, int par, const PhysT<T> &p,
+                                            T rka, T rkbdt, unsigned char *smem) {
+  using C = BCfg<DIM, Nq, G>;
+  constexpr int NS = Lay<DIM>::NS, NVG = Lay<DIM>::NVG, NSG = Lay<DIM>::NSG, IR = Lay<DIM>::IR;
+  constexpr int Np = C::Np, Nfp = C::Nfp, NF = C::NFACE, SP = C::SLOTS, FS = C::EPB * Nfp;
+  constexpr int MJI = DIM * DIM + 1, GC = DIM * DIM + 2 + DIM - 1;
+  const T *__restrict__ Qin = I.Q[par];
+  T *__restrict__ Qout = I.Q[par ^ 1];
+  T *__restrict__ rhs = I.rhs;
+  const T *__restrict__ vgeo = I.vgeo;
+  T *Ds = reinterpret_cast<T *>(smem);
+  T *sQ = Ds + ((Nq * Nq + 1) & ~1);  // [NS][SP]
+  T *sF = sQ + NS * SP;               // [DIM][NS][SP], reused as the face buffer
+  for (int t = threadIdx.x; t < Nq * Nq; t += BT) Ds[t] = I.D[t];
+  T R[C::NPT][NS];
+  // ---- pointwise contravariant fluxes
+#pragma unroll
+  for (int u = 0; u < C::NPT; ++u) {
+    const int slot = threadIdx.x + u * BT;
+    const int el = slot / Np, n = slot % Np;
+    const int64_t e = e0 + el;
+    if (slot < SP && el < nv) {
+      T q[NS];
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        const T d = Qin[n + Np * (s + NS * e)];
+        sQ[s * SP + slot] = d;
+        q[s] = d + I.qref[s];
+        R[u][s] = rhs[n + Np * (s + NS * e)];
+      }
+      const T *vg = vgeo + (int64_t)Np * NVG * e;
+      T met[DIM][DIM], MJ;
+      load_metric<DIM, T>(vg, n, Np, met, MJ);
+      const T gc = p.grav != T(0) ? vg[n + Np * GC] : T(0);
+      const T ri = T(1) / q[IR];
+      const T P = pressure_ri<DIM, T>(q, ri, gc, p);
+      T f[NS][DIM];
+      euler_flux_ri<DIM, T>(q, ri, P, f);
+#pragma unroll
+      for (int r = 0; r < DIM; ++r)
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+          T a = met[r][0] * f[s][0] + met[r][1] * f[s][1];
+          if (DIM == 3) a = a + met[r][2] * f[s][2];
+          sF[(r * NS + s) * SP + el * Np + n] = MJ * a;
+        }
+      R[u][DIM - 1] -= MJ * q[IR] * p.grav;
+    }
+  }
+  __syncthreads();
+  // ---- volume contraction
+#pragma unroll
+  for (int u = 0; u < C::NPT; ++u) {
+    const int slot = threadIdx.x + u * BT;
+    const int el = slot / Np, n = slot % Np;
+    if (slot < SP && el < nv) contract<DIM, Nq, C::EPB, T>(sF, Ds, el, n, R[u]);
+  }
+  __syncthreads();
+  // ---- face fluxes into FF[NF][NS][EPB*Nfp] (aliases sF)
+  T *FF = sF;
+#pragma unroll
+  for (int u = 0; u < C::FPT; ++u) {
+    const int fs = threadIdx.x + u * BT;
+    if (fs >= C::FSLOTS) break;
+    const int el = fs / (NF * Nfp), f = (fs / Nfp) % NF, fn = fs % Nfp;
+    const int64_t e = e0 + el;
+    if (el >= nv) continue;
+    const int vM = face_node<DIM, Nq>(f, fn);
+    const T *sg = I.sgeo + (int64_t)NSG * (fn + (int64_t)Nfp * (f + NF * e));
+    T nrm[DIM];
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) nrm[c] = sg[c];
+    const T smj = sg[DIM];
+    T qM[NS], qP[NS];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) qM[s] = sQ[s * SP + el * Np + vM] + I.qref[s];
+    const T gM = p.grav != T(0) ? vgeo[vM + Np * (GC + NVG * e)] : T(0);
+    const T riM = T(1) / qM[IR];
+    const T PM = pressure_ri<DIM, T>(qM, riM, gM, p);
+    const int32_t nb = I.nbr[f + NF * e];
+    T PP, riP;
+    if (nb >= 0) {
+      const int64_t e2 = nb >> 3;
+      const int vP = face_node<DIM, Nq>(nb & 7, fn);
+#pragma unroll
+      for (int s = 0; s < NS; ++s) qP[s] = Qin[vP + Np * (s + NS * e2)] + I.qref[s];
+      const T gP = p.grav != T(0) ? vgeo[vP + Np * (GC + NVG * e2)] : T(0);
+      riP = T(1) / qP[IR];
+      PP = pressure_ri<DIM, T>(qP, riP, gP, p);
+    } else {
+      wall_state<DIM, T>(qM, nrm, qP);
+      riP = riM;
+      PP = PM;
+    }
+    T out[NS];
+    rusanov_n<DIM, T>(qM, riM, PM, qP, riP, PP, nrm, p, out);
+#pragma unroll
+    for (int s = 0; s < NS; ++s) FF[(f * NS + s) * FS + el * Nfp + fn] = smj * out[s];
+  }
+  __syncthreads();
+  // ---- face accumulation and LSRK update
+  bool bad = false;
+#pragma unroll
+  for (int u = 0; u < C::NPT; ++u) {
+    const int slot = threadIdx.x + u * BT;
+    const int el = slot / Np, n = slot % Np;
+    const int64_t e = e0 + el;
+    if (slot < SP && el < nv) {
+      gather_face_terms<DIM, Nq, C::EPB, T>(FF, el, n, R[u]);
+      const T mji = vgeo[n + Np * (MJI + (int64_t)NVG * e)];
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        const T qn = sQ[s * SP + slot] + rkbdt * R[u][s] * mji;
+        bad |= !isfinite(qn);
+        Qout[n + Np * (s + NS * e)] = qn;
+        rhs[n + Np * (s + NS * e)] = R[u][s] * rka;
+      }
+    }
+  }
+  if (bad) atomicOr(I.status, ST_NONFINITE);
+  __syncthreads();  // shared memory is reused by the block's next item
+}
+
+// Persistent grouped stage kernel of one shape: the blocks stride over the
+// shape's work list.
+template <int DIM, int Nq, int G, typename T>
+__global__ void __launch_bounds__(BT, 2)
+k_stage_batch(const BHdr *__restrict__ hdr, int stage, PhysT<T> p, T rka, double rkb) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int SID = shape_id(DIM, Nq - 1, 1 + G);
+  const int nwork = hdr->nwork[SID];
+  const int64_t step = hdr->step;
+  const BWork *__restrict__ work = hdr->work[SID];
+  const BDesc<T> *__restrict__ desc = static_cast<const BDesc<T> *>(hdr->desc);
+  for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+    const BWork it = work[w];
+    if (!it.valid) continue;  // uniform over the block
+    const BDesc<T> &I = desc[it.slot];
+    const int64_t k = step - I.start;
+    if (k >= I.target) continue;
+    stage_group<DIM, Nq, G, T>(I, it.e0, it.nv, (int)((k + stage) & 1), p, rka, T(rkb * I.dt), smem_raw);
+  }
+}
+
+// Item source of the pipelined stage over a work list of many instances
+// (see k_stage_pipe2).  The second warp of the block (the first issues the
+// bulk copies) finds the block's next live item and publishes it into a
+// three-entry shared-memory ring (current, next, and the one being published):
+// each lane copies one 8-byte word of the instance descriptor, so a publish
+// costs two parallel round trips (work item, descriptor).  The shape's list,
+// the descriptor table and the batch step are cached at the head of the ring.
+template <typename T>
+struct BItem {
+  BDesc<T> d;  // word-for-word copy of the instance descriptor
+  int64_t e0;
+  int32_t nv, valid, par, pad;
+};
+struct alignas(16) BRingHdr {
+  const BWork *work;
+  const void *desc;
+  int64_t step;
+  int32_t nwork, pad;
+};
+template <typename T, int NS, int EPB>
+struct BatchSrc {
+  static constexpr int WORDS = (int)(sizeof(BDesc<T>) / 8);
+  static_assert(sizeof(BDesc<T>) % 8 == 0 && WORDS <= 32, "descriptor words");
+  static constexpr int START_WORD = (int)(offsetof(BDesc<T>, start) / 8);
+  static constexpr int TARGET_WORD = (int)(offsetof(BDesc<T>, target) / 8);
+  static constexpr size_t RING_BYTES = sizeof(BRingHdr) + 3 * sizeof(BItem<T>);
+  static constexpr int PUBLISHER = 32;  // first thread of the publishing warp
+  const BHdr *hdr;
+  int sid, stage;
+  double rkb;
+  BRingHdr *rh;
+  BItem<T> *ring;
+  int wpos;  // publishing warp: work index of the last published item (-1: none)
+
+  // whole publishing warp: publish the first live item at or after w on this
+  // block's stride into dst; returns its index (-1: none)
+  __device__ int publish_from(int w, BItem<T> &dst) const {
+    const int lane = threadIdx.x & 31;
+    const BWork *work = rh->work;
+    const int nwork = rh->nwork;
+    const int64_t step = rh->step;
+    const unsigned long long *dw = static_cast<const unsigned long long *>(rh->desc);
+    for (; w >= 0 && w < nwork; w += gridDim.x) {
+      const BWork wk = work[w];
+      if (!wk.valid) continue;
+      const unsigned long long v = lane < WORDS ? dw[(size_t)wk.slot * WORDS + lane] : 0ull;
+      const int64_t start = (int64_t)__shfl_sync(0xffffffffu, v, START_WORD);
+      const int64_t target = (int64_t)__shfl_sync(0xffffffffu, v, TARGET_WORD);
+      if (step - start >= target) continue;
+      if (lane < WORDS) reinterpret_cast<unsigned long long *>(&dst.d)[lane] = v;
+      if (lane == 0) {
+        dst.e0 = wk.e0;
+        dst.nv = wk.nv;
+        dst.par = (int)((step - start + stage) & 1);
+        dst.valid = 1;
+      }
+      return w;
+    }
+    if (lane == 0) dst.valid = 0;
+    return -1;
+  }
+  __device__ void begin(unsigned char *mem) {
+    rh = reinterpret_cast<BRingHdr *>(mem);
+    ring = reinterpret_cast<BItem<T> *>(mem + sizeof(BRingHdr));
+    if ((threadIdx.x >> 5) == (PUBLISHER >> 5)) {
+      if ((threadIdx.x & 31) == 0) {
+        rh->work = hdr->work[sid];
+        rh->desc = hdr->desc;
+        rh->step = hdr->step;
+        rh->nwork = hdr->nwork[sid];
+      }
+      __syncwarp();
+      const int w0 = publish_from(blockIdx.x, ring[0]);
+      const int w1 = w0 < 0 ? -1 : publish_from(w0 + gridDim.x, ring[1]);
+      wpos = w1;
+    }
+  }
+  // start fetching the work item that publish() will most likely read (the
+  // next one on this block's stride), so that its cache miss overlaps the wait
+  // for the current group's bulk copies
+  __device__ void prefetch() const {
+    const int w = wpos < 0 ? -1 : wpos + (int)gridDim.x;
+    if (w < 0 || w >= rh->nwork) return;
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(rh->work + w));
+  }
+  __device__ void publish(int it) {
+    wpos = wpos < 0 ? -1 : publish_from(wpos + gridDim.x, ring[(it + 2) % 3]);
+    if (wpos < 0 && (threadIdx.x & 31) == 0) ring[(it + 2) % 3].valid = 0;
+  }
+  __device__ const BItem<T> &at(int it) const { return ring[it % 3]; }
+  __device__ bool valid(int it) const { return at(it).valid != 0; }
+  __device__ int64_t e0(int it) const { return at(it).e0; }
+  __device__ int nv(int it) const { return at(it).nv; }
+  __device__ const T *Qin(int it) const { return at(it).d.Q[at(it).par]; }
+  __device__ T *Qout(int it) const { return at(it).d.Q[at(it).par ^ 1]; }
+  __device__ T *rhs(int it) const { return at(it).d.rhs; }
+  __device__ const T *vgeo(int it) const { return at(it).d.vgeo; }
+  __device__ const T *sgeo(int it) const { return at(it).d.sgeo; }
+  __device__ const int32_t *nbr(int it) const { return at(it).d.nbr; }
+  __device__ const T *D(int it) const { return at(it).d.D; }
+  __device__ T qref(int it, int s) const { return at(it).d.qref[s]; }
+  __device__ T rkbdt(int it) const { return T(rkb * at(it).d.dt); }
+  __device__ unsigned *status(int it) const { return at(it).d.status; }
+};
+template <int DIM, int Nq, typename T>
+using BPipeSrc = BatchSrc<T, Lay<DIM>::NS, Cfg<DIM, Nq>::EPB>;
+
+inline bool b_order_ok(int dim, int N) { return N >= 1 && N <= (dim == 2 ? BMAXN2 : BMAXN3); }
+
+// Host table of the stage kernels of one precision, indexed by shape id:
+// kernel, elements per group, threads, dynamic shared memory, whether the
+// kernel is the pipelined one, and its persistent grid once prepared.
+template <typename T>
+struct BKernels {
+  const void *fn[NSHAPE] = {};
+  int epb[NSHAPE] = {}, threads[NSHAPE] = {}, grid[NSHAPE] = {};
+  size_t smem[NSHAPE] = {};
+  bool pipelined[NSHAPE] = {}, ready[NSHAPE] = {};
+};
+template <int DIM, int Nq, int G, typename T>
+constexpr size_t b_group_smem() {
+  using C = BCfg<DIM, Nq, G>;
+  return sizeof(T) * (((Nq * Nq + 1) & ~1) + (size_t)Lay<DIM>::NS * C::SLOTS +
+                      (size_t)DIM * Lay<DIM>::NS * C::SLOTS);
+}
+template <int DIM, int Nq, typename T, int MINB>
+void b_fill_pipe(BKernels<T> &k, int var) {
+  const int id = shape_id(DIM, Nq - 1, var);
+  k.fn[id] = (const void *)k_stage_pipe2<DIM, Nq, T, BPipeSrc<DIM, Nq, T>, MINB>;
+  k.epb[id] = Cfg<DIM, Nq>::EPB;
+  k.threads[id] = Cfg<DIM, Nq>::THREADS;
+  k.smem[id] = Pipe2<DIM, Nq, T>::smem() + BPipeSrc<DIM, Nq, T>::RING_BYTES;
+  k.pipelined[id] = true;
+}
+template <int DIM, int Nq, typename T>
+void b_fill(BKernels<T> &k) {
+  constexpr int N = Nq - 1;
+  if constexpr (Pipe2<DIM, Nq, T>::OK) {
+    constexpr int M0 = Pipe2<DIM, Nq, T>::MINB;
+    b_fill_pipe<DIM, Nq, T, M0>(k, 0);
+    // blocks of up to 256 threads: also sized for three and four per SM
+    if constexpr (Cfg<DIM, Nq>::THREADS <= 256) {
+      b_fill_pipe<DIM, Nq, T, M0 == 3 ? 2 : 3>(k, 3);
+      b_fill_pipe<DIM, Nq, T, M0 == 4 ? 2 : 4>(k, 4);
+    }
+  }
+  {
+    const int id = shape_id(DIM, N, 1);
+    k.fn[id] = (const void *)k_stage_batch<DIM, Nq, 0, T>;
+    k.epb[id] = BCfg<DIM, Nq, 0>::EPB;
+    k.threads[id] = BT;
+    k.smem[id] = b_group_smem<DIM, Nq, 0, T>();
+  }
+  if constexpr (BCfg<DIM, Nq, 1>::OK) {
+    const int id = shape_id(DIM, N, 2);
+    k.fn[id] = (const void *)k_stage_batch<DIM, Nq, 1, T>;
+    k.epb[id] = BCfg<DIM, Nq, 1>::EPB;
+    k.threads[id] = BT;
+    k.smem[id] = b_group_smem<DIM, Nq, 1, T>();
+  }
+}
+// Fill the table entries of one dimension (one translation unit per
+// dimension and precision instantiates the kernels).
+template <int DIM, typename T>
+void b_fill_dim(BKernels<T> &k);
+
+}  // namespace cb

@@ -802,14 +802,21 @@ struct Launch {
     const bool aligned2 = aligned && ((reinterpret_cast<uintptr_t>(rhs) | reinterpret_cast<uintptr_t>(sgeo)) & 15) == 0;
     if (Pipe2<DIM, Nq, T>::OK && aligned2) {
       using PP = Pipe2<DIM, Nq, T>;
-      size_t sm = PP::smem();
-      cudaError_t err = prep(k_stage_pipe2<DIM, Nq, T>, sm);
-      if (err != cudaSuccess) return err;
+      using S = MeshSrc<T, NS, C::EPB>;
+      const size_t sm = PP::smem();
+      static int per_sm = 0;  // resident blocks per SM, from the occupancy calculator
+      if (!per_sm) {
+        cudaError_t err = prep(k_stage_pipe2<DIM, Nq, T, S>, sm);
+        if (err != cudaSuccess) return err;
+        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stage_pipe2<DIM, Nq, T, S>, C::THREADS, sm);
+        if (err != cudaSuccess) return err;
+        if (per_sm < 1) per_sm = 1;
+      }
       const int64_t groups = (nelem + C::EPB - 1) / C::EPB;
-      int g = num_sms();
-      if ((int64_t)g > groups) g = (int)groups;
-      k_stage_pipe2<DIM, Nq, T><<<g, C::THREADS, sm, st>>>(Qin, Qout, rhs, vgeo, sgeo, nbr, D, nelem,
-                                                           p, qref, rka, rkbdt, status);
+      int64_t g = (int64_t)num_sms() * per_sm;
+      if (g > groups) g = groups;
+      const S src{Qin, Qout, rhs, vgeo, sgeo, nbr, D, nelem, qref, rkbdt, status};
+      k_stage_pipe2<DIM, Nq, T, S><<<(int)g, C::THREADS, sm, st>>>(src, p, rka);
       return cudaGetLastError();
     } else if (pipe_ok && aligned) {
       using PP = Pipe<DIM, Nq, T>;

@@ -11,6 +11,18 @@
 //     one group ahead.
 // Used when every slab is a multiple of 16 bytes (bulk copies) and the
 // shared-memory plan fits; otherwise k_stage_pipe / k_stage are used.
+//
+// The kernel walks a sequence of element groups given by a source policy
+// `Src`: MeshSrc is one mesh (group g of block b at iteration it is
+// b + it * gridDim.x, all pointers kernel parameters); the batched driver
+// supplies a source whose groups come from a work list over many instances,
+// with per-group pointers published by one thread into a small shared-memory
+// ring.  A source provides, for the block's iteration `it`:
+//   valid(it), e0(it), nv(it) (elements in the group), Qin/Qout/rhs/vgeo/
+//   sgeo/nbr/D(it), qref(it, s), rkbdt(it), status(it);
+// begin(ring) (all threads, before the first barrier), prefetch() (thread
+// PUBLISHER, at the top of each iteration) and publish(it) (the warp of
+// thread PUBLISHER, during phase B of iteration it, for iteration it + 2).
 #pragma once
 
 namespace cb {
@@ -19,15 +31,20 @@ template <int DIM, int Nq, typename T>
 struct Pipe2 {
   using C = Cfg<DIM, Nq>;
   using P1 = Pipe<DIM, Nq, T>;
-  static constexpr int NS = Lay<DIM>::NS, NSG = Lay<DIM>::NSG;
+  static constexpr int NS = Lay<DIM>::NS, NSG = Lay<DIM>::NSG, NVG = Lay<DIM>::NVG;
   static constexpr int NG = P1::NG, RS = P1::RS, NR = P1::NR, MV = P1::MV;
   static constexpr size_t QB = P1::QB, GB = P1::GB;
-  static constexpr size_t SB = sizeof(T) * (size_t)NSG * C::Nfp * C::NFACE;  // sgeo per element
-  static constexpr bool BULK = P1::BULK && SB % 16 == 0;
   static constexpr size_t pad16(size_t b) { return (b + 15) & ~size_t(15); }
+  // the metric fields of an element are copied as one padded run (the pad
+  // reads the start of the coordinate fields, which are never used)
+  static constexpr size_t GBP = pad16(GB);
+  static constexpr int GS = (int)(GBP / sizeof(T));  // element stride of the staged metric
+  static constexpr size_t VB = sizeof(T) * (size_t)C::Np * NVG;  // vgeo bytes per element
+  static constexpr size_t SB = sizeof(T) * (size_t)NSG * C::Nfp * C::NFACE;  // sgeo per element
+  static constexpr bool BULK = QB % 16 == 0 && VB % 16 == 0 && SB % 16 == 0 && GBP <= VB;
   static constexpr size_t OFF_D = 32;  // 3 mbarriers before
   static constexpr size_t OFF_S = OFF_D + pad16(sizeof(T) * Nq * RS);
-  static constexpr size_t SBYTES = C::EPB * (QB + GB);
+  static constexpr size_t SBYTES = C::EPB * (QB + GBP);
   static constexpr size_t OFF_T = OFF_S + pad16(SBYTES);
   static constexpr size_t TBYTES = C::EPB * (QB + SB);
   static constexpr size_t OFF_F = OFF_T + 2 * pad16(TBYTES);
@@ -35,100 +52,143 @@ struct Pipe2 {
   static constexpr size_t FLUX = sizeof(T) * DIM * FDIR;
   static constexpr size_t OFF_FF = OFF_F + pad16(FLUX);
   static constexpr size_t FFB = P1::FFB;
-  static constexpr size_t smem() { return OFF_FF + FFB; }
-  static constexpr bool OK = BULK && smem() <= SMEM_LIMIT;
+  static constexpr size_t smem() { return OFF_FF + pad16(FFB); }  // sources append their ring here
+  static constexpr size_t RING_MAX = 640;
+  static constexpr bool OK = BULK && smem() + RING_MAX <= SMEM_LIMIT;
+  // blocks of up to 256 threads are sized for two (FP64) or four (FP32) per SM
+  static constexpr int MINB = C::THREADS <= 256 ? (sizeof(T) == 4 ? 4 : 2) : 1;
 };
 
-template <int DIM, int Nq, typename T>
-__global__ void __launch_bounds__(Cfg<DIM, Nq>::THREADS, 1)
-k_stage_pipe2(const T *__restrict__ Qin, T *__restrict__ Qout, T *__restrict__ rhs,
-              const T *__restrict__ vgeo, const T *__restrict__ sgeo,
-              const int32_t *__restrict__ nbr, const T *__restrict__ D, int64_t nelem,
-              PhysT<T> p, Offs<T, Lay<DIM>::NS> qref, T rka, T rkbdt, unsigned *status) {
+// One mesh: groups of EPB consecutive elements, pointers and constants are
+// kernel parameters.
+template <typename T, int NS, int EPB>
+struct MeshSrc {
+  static constexpr size_t RING_BYTES = 0;
+  static constexpr int PUBLISHER = 0;
+  const T *Qin_;
+  T *Qout_, *rhs_;
+  const T *vgeo_, *sgeo_;
+  const int32_t *nbr_;
+  const T *D_;
+  int64_t nelem;
+  Offs<T, NS> qref_;
+  T rkbdt_;
+  unsigned *status_;
+  __device__ void begin(unsigned char *) {}
+  __device__ void prefetch() {}
+  __device__ void publish(int) {}
+  __device__ int64_t g(int it) const { return (int64_t)blockIdx.x + (int64_t)it * gridDim.x; }
+  __device__ bool valid(int it) const { return g(it) * EPB < nelem; }
+  __device__ int64_t e0(int it) const { return g(it) * EPB; }
+  __device__ int nv(int it) const {
+    const int64_t r = nelem - e0(it);
+    return r < EPB ? (int)r : EPB;
+  }
+  __device__ const T *Qin(int) const { return Qin_; }
+  __device__ T *Qout(int) const { return Qout_; }
+  __device__ T *rhs(int) const { return rhs_; }
+  __device__ const T *vgeo(int) const { return vgeo_; }
+  __device__ const T *sgeo(int) const { return sgeo_; }
+  __device__ const int32_t *nbr(int) const { return nbr_; }
+  __device__ const T *D(int) const { return D_; }
+  __device__ T qref(int, int s) const { return qref_.v[s]; }
+  __device__ T rkbdt(int) const { return rkbdt_; }
+  __device__ unsigned *status(int) const { return status_; }
+};
+
+// MINB: resident blocks per SM that the register allocation is sized for.
+template <int DIM, int Nq, typename T, typename Src, int MINB = Pipe2<DIM, Nq, T>::MINB>
+__global__ void __launch_bounds__(Cfg<DIM, Nq>::THREADS, MINB)
+k_stage_pipe2(Src src, PhysT<T> p, T rka) {
   using C = Cfg<DIM, Nq>;
   using PP = Pipe2<DIM, Nq, T>;
   constexpr int NS = Lay<DIM>::NS, NVG = Lay<DIM>::NVG, NSG = Lay<DIM>::NSG, IR = Lay<DIM>::IR;
   constexpr int Np = C::Np, Nfp = C::Nfp, NF = C::NFACE, EPB = C::EPB, SP = C::SLOTS;
-  constexpr int NG = PP::NG, MJI = DIM * DIM + 1, GC = DIM * DIM + 2 + DIM - 1;
-  constexpr int FS = EPB * Nfp, RS = PP::RS, NR = PP::NR;
+  constexpr int MJI = DIM * DIM + 1, GC = DIM * DIM + 2 + DIM - 1;
+  constexpr int FS = EPB * Nfp, RS = PP::RS, NR = PP::NR, GS = PP::GS;
   constexpr size_t TSTRIDE = PP::pad16(PP::TBYTES) / sizeof(T);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   uint64_t *barS = reinterpret_cast<uint64_t *>(smem_raw);
   uint64_t *barT = barS + 1;  // barT[0], barT[1]
   T *DT = reinterpret_cast<T *>(smem_raw + PP::OFF_D);
   T *Sq = reinterpret_cast<T *>(smem_raw + PP::OFF_S);  // [EPB][NS][Np]
-  T *Sg = Sq + EPB * Np * NS;                             // [EPB][NG][Np]
+  T *Sg = Sq + EPB * Np * NS;                             // [EPB][GS]: metric, MJ, MJI rows
   T *T0 = reinterpret_cast<T *>(smem_raw + PP::OFF_T);   // [EPB][NS][Np] carry, then [EPB] sgeo
   T *sF = reinterpret_cast<T *>(smem_raw + PP::OFF_F);
   T *FF = reinterpret_cast<T *>(smem_raw + PP::OFF_FF);
   const int tid = threadIdx.x;
-  const int64_t ngroups = (nelem + EPB - 1) / EPB;
 
-  auto nvalid = [&](int64_t g) { return (int)((nelem - g * EPB) < EPB ? (nelem - g * EPB) : EPB); };
-  auto issue_S = [&](int64_t g) {  // thread 0 only
-    const int64_t e0 = g * EPB;
-    const int nv = nvalid(g);
+  auto issue_S = [&](int it) {  // thread 0 only
+    const int64_t e0 = src.e0(it);
+    const int nv = src.nv(it);
+    const T *q = src.Qin(it), *vg = src.vgeo(it);
     fence_proxy_async();
-    mbar_expect_tx(barS, (uint32_t)(nv * (PP::QB + PP::GB)));
-    bulk_g2s(Sq, Qin + e0 * Np * NS, (uint32_t)(nv * PP::QB), barS);
+    mbar_expect_tx(barS, (uint32_t)(nv * (PP::QB + PP::GBP)));
+    bulk_g2s(Sq, q + e0 * Np * NS, (uint32_t)(nv * PP::QB), barS);
     for (int el = 0; el < nv; ++el)
-      bulk_g2s(Sg + el * Np * NG, vgeo + (e0 + el) * Np * NVG, (uint32_t)PP::GB, barS);
+      bulk_g2s(Sg + el * GS, vg + (e0 + el) * Np * NVG, (uint32_t)PP::GBP, barS);
   };
-  auto issue_T = [&](int64_t g, int b) {  // thread 0 only
-    const int64_t e0 = g * EPB;
-    const int nv = nvalid(g);
+  auto issue_T = [&](int it, int b) {  // thread 0 only
+    const int64_t e0 = src.e0(it);
+    const int nv = src.nv(it);
     T *dc = T0 + b * TSTRIDE, *ds = dc + EPB * Np * NS;
     fence_proxy_async();
     mbar_expect_tx(&barT[b], (uint32_t)(nv * (PP::QB + PP::SB)));
-    bulk_g2s(dc, rhs + e0 * Np * NS, (uint32_t)(nv * PP::QB), &barT[b]);
-    bulk_g2s(ds, sgeo + e0 * (PP::SB / sizeof(T)), (uint32_t)(nv * PP::SB), &barT[b]);
+    bulk_g2s(dc, src.rhs(it) + e0 * Np * NS, (uint32_t)(nv * PP::QB), &barT[b]);
+    bulk_g2s(ds, src.sgeo(it) + e0 * (PP::SB / sizeof(T)), (uint32_t)(nv * PP::SB), &barT[b]);
   };
 
+  src.begin(smem_raw + PP::smem());
   if (tid == 0) {
     mbar_init(barS, 1);
     mbar_init(&barT[0], 1);
     mbar_init(&barT[1], 1);
     fence_mbar_init();
   }
-  for (int t = tid; t < Nq * RS; t += C::THREADS) {
-    const int i = t / RS, m = t % RS;
-    DT[t] = m < Nq ? D[m + Nq * i] : T(0);
-  }
   if constexpr (PP::MV > Nq)
     for (size_t t = tid; t < (size_t)DIM * PP::FDIR; t += C::THREADS)
       if ((int)(t % RS) >= Nq) sF[t] = T(0);
   __syncthreads();
-  if (tid == 0 && (int64_t)blockIdx.x < ngroups) {
-    issue_S(blockIdx.x);
-    issue_T(blockIdx.x, 0);
+  if (tid == 0 && src.valid(0)) {
+    issue_S(0);
+    issue_T(0, 0);
   }
 
   int32_t nbn[C::FPT];
-  auto load_nbr = [&](int64_t g, int32_t *dst) {
+  auto load_nbr = [&](int it, int32_t *dst) {
+    const bool ok = src.valid(it);
+    const int64_t e0 = ok ? src.e0(it) : 0;
+    const int nv = ok ? src.nv(it) : 0;
+    const int32_t *nb = src.nbr(it);
 #pragma unroll
     for (int u = 0; u < C::FPT; ++u) {
       const int fs = tid + u * C::THREADS;
       const int el = fs / (NF * Nfp), f = (fs / Nfp) % NF;
-      const int64_t e = g * EPB + el;
-      dst[u] = (g < ngroups && fs < C::FSLOTS && e < nelem) ? nbr[f + NF * e] : NBR_WALL;
+      dst[u] = (fs < C::FSLOTS && el < nv) ? nb[f + NF * (e0 + el)] : NBR_WALL;
     }
   };
-  load_nbr(blockIdx.x, nbn);
+  load_nbr(0, nbn);
 
-  bool bad = false, timed_out = false;
-  int it = 0;
-  for (int64_t g = blockIdx.x; g < ngroups; g += gridDim.x, ++it) {
+  bool timed_out = false;
+  const T *curD = nullptr;  // derivative matrix held in DT (rows padded like the flux rows)
+  for (int it = 0; src.valid(it); ++it) {
     const int b = it & 1;
-    const int64_t e0 = g * EPB;
-    const int64_t gn = g + gridDim.x;
-    if (tid == 0 && gn < ngroups) issue_T(gn, b ^ 1);
+    const int64_t e0 = src.e0(it);
+    const int nv = src.nv(it);
+    const bool more = src.valid(it + 1);
+    if (tid == 0 && more) issue_T(it + 1, b ^ 1);
+    if (tid == Src::PUBLISHER) src.prefetch();
+    const T *__restrict__ Qin = src.Qin(it);
+    T qr[NS];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) qr[s] = src.qref(it, s);
 
     // ---- neighbour traces of this group (codes were loaded one group ago)
     T qP[C::FPT][NS];
     int32_t nbv[C::FPT];
 #pragma unroll
     for (int u = 0; u < C::FPT; ++u) nbv[u] = nbn[u];
-    load_nbr(gn, nbn);
+    load_nbr(it + 1, nbn);
 #pragma unroll
     for (int u = 0; u < C::FPT; ++u) {
       const int fs = tid + u * C::THREADS;
@@ -137,7 +197,7 @@ k_stage_pipe2(const T *__restrict__ Qin, T *__restrict__ Qout, T *__restrict__ r
         const int64_t e2 = nbv[u] >> 3;
         const int vP = face_node<DIM, Nq>(nbv[u] & 7, fn);
 #pragma unroll
-        for (int s = 0; s < NS; ++s) qP[u][s] = Qin[vP + Np * (s + NS * e2)] + qref.v[s];
+        for (int s = 0; s < NS; ++s) qP[u][s] = Qin[vP + Np * (s + NS * e2)] + qr[s];
       }
     }
 
@@ -145,6 +205,14 @@ k_stage_pipe2(const T *__restrict__ Qin, T *__restrict__ Qout, T *__restrict__ r
     if (!mbar_wait_bounded(barS, (uint32_t)(it & 1), WAIT_LIMIT)) timed_out = true;
     if (!mbar_wait_bounded(&barT[b], (uint32_t)((it >> 1) & 1), WAIT_LIMIT)) timed_out = true;
     const T *Tc = T0 + b * TSTRIDE, *Ts = Tc + EPB * Np * NS;
+    const T *__restrict__ vgeo = src.vgeo(it);
+    if (src.D(it) != curD) {  // read in phase B only; visible after the mid barrier
+      curD = src.D(it);
+      for (int t = tid; t < Nq * RS; t += C::THREADS) {
+        const int i = t / RS, m = t % RS;
+        DT[t] = m < Nq ? curD[m + Nq * i] : T(0);
+      }
+    }
 
     // ---- phase A: volume fluxes (state and 1/MJ kept in registers) and face fluxes
     T qd[C::NPT][NS], mji[C::NPT], buoy[C::NPT];
@@ -154,20 +222,21 @@ k_stage_pipe2(const T *__restrict__ Qin, T *__restrict__ Qout, T *__restrict__ r
       const int el = slot / Np, n = slot % Np;
       buoy[u] = T(0);
       mji[u] = T(0);
-      if (slot < SP && e0 + el < nelem) {
+      if (slot < SP && el < nv) {
         T q[NS];
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
           qd[u][s] = Sq[(el * NS + s) * Np + n];
-          q[s] = qd[u][s] + qref.v[s];
+          q[s] = qd[u][s] + qr[s];
         }
+        const T *G = Sg + el * GS;
         T met[DIM][DIM];
 #pragma unroll
         for (int r = 0; r < DIM; ++r)
 #pragma unroll
-          for (int c = 0; c < DIM; ++c) met[r][c] = Sg[(el * NG + r + DIM * c) * Np + n];
-        const T MJ = Sg[(el * NG + DIM * DIM) * Np + n];
-        mji[u] = Sg[(el * NG + MJI) * Np + n];
+          for (int c = 0; c < DIM; ++c) met[r][c] = G[(r + DIM * c) * Np + n];
+        const T MJ = G[DIM * DIM * Np + n];
+        mji[u] = G[MJI * Np + n];
         const T gc = p.grav != T(0) ? vgeo[n + Np * (GC + NVG * (e0 + el))] : T(0);
         const T ri = T(1) / q[IR];
         const T P = pressure_ri<DIM, T>(q, ri, gc, p);
@@ -192,7 +261,7 @@ k_stage_pipe2(const T *__restrict__ Qin, T *__restrict__ Qout, T *__restrict__ r
     for (int u = 0; u < C::FPT; ++u) {
       const int fs = tid + u * C::THREADS;
       const int el = fs / (NF * Nfp), f = (fs / Nfp) % NF, fn = fs % Nfp;
-      if (fs < C::FSLOTS && e0 + el < nelem) {
+      if (fs < C::FSLOTS && el < nv) {
         const T *sg = Ts + (size_t)NSG * (fn + Nfp * (f + NF * el));
         T nrm[DIM];
 #pragma unroll
@@ -201,7 +270,7 @@ k_stage_pipe2(const T *__restrict__ Qin, T *__restrict__ Qout, T *__restrict__ r
         const int vM = face_node<DIM, Nq>(f, fn);
         T qM[NS], qq[NS];
 #pragma unroll
-        for (int s = 0; s < NS; ++s) qM[s] = Sq[(el * NS + s) * Np + vM] + qref.v[s];
+        for (int s = 0; s < NS; ++s) qM[s] = Sq[(el * NS + s) * Np + vM] + qr[s];
         const T gM = p.grav != T(0) ? vgeo[vM + Np * (GC + NVG * (e0 + el))] : T(0);
         const T riM = T(1) / qM[IR];
         const T PM = pressure_ri<DIM, T>(qM, riM, gM, p);
@@ -229,14 +298,19 @@ k_stage_pipe2(const T *__restrict__ Qin, T *__restrict__ Qout, T *__restrict__ r
     }
     __syncthreads();
     // S is no longer read: refill it with the next group while phase B runs
-    if (tid == 0 && gn < ngroups) issue_S(gn);
+    if (tid == 0 && more) issue_S(it + 1);
+    if ((tid >> 5) == (Src::PUBLISHER >> 5)) src.publish(it);
     // ---- phase B: carry - source + volume contraction - face terms, update
+    T *__restrict__ Qout = src.Qout(it);
+    T *__restrict__ rhs = src.rhs(it);
+    const T rkbdt = src.rkbdt(it);
+    bool bad = false;
 #pragma unroll
     for (int u = 0; u < C::NPT; ++u) {
       const int slot = tid + u * C::THREADS;
       const int el = slot / Np, n = slot % Np;
       const int64_t e = e0 + el;
-      if (slot < SP && e < nelem) {
+      if (slot < SP && el < nv) {
         T R[NS];
 #pragma unroll
         for (int s = 0; s < NS; ++s) R[s] = Tc[(el * NS + s) * Np + n];
@@ -252,10 +326,13 @@ k_stage_pipe2(const T *__restrict__ Qin, T *__restrict__ Qout, T *__restrict__ r
         }
       }
     }
-    __syncthreads();  // T[b], the flux rows and FF are free for reuse
+    if (bad) atomicOr(src.status(it), ST_NONFINITE);
+    if (timed_out) {
+      atomicOr(src.status(it), ST_TIMEOUT);
+      timed_out = false;
+    }
+    __syncthreads();  // T[b], the flux rows, FF and the item ring are free for reuse
   }
-  if (bad) atomicOr(status, ST_NONFINITE);
-  if (timed_out) atomicOr(status, ST_TIMEOUT);
 }
 
 }  // namespace cb
