@@ -160,6 +160,52 @@ def cpu_sample(N, seconds=10.0, n_side=16, max_steps=40):
                       f"({5 * steps} stages) in {el:.1f} s, C oracle with {cores} OpenMP threads"}
 
 
+def batched_ensemble(count=512, seed=0, steps=500, device="cuda"):
+    """The batched workload: `count` independent 2-D vortex instances (N, mesh,
+    strength and centre drawn per instance from PCG64(seed + i)), dt = 0.002,
+    `steps` LSRK(5,4) steps each, advanced together by one Batch per precision
+    (one graph launch per step).  Returns throughput, solves/s and the FP32
+    form's relative L2 error per field against the FP64 batch."""
+    import torch
+    from canary_b200 import batch as B, ic
+    params = ic.vortex_ensemble(count, seed)
+    cache = B.MeshCache(device)
+    t0 = time.time()
+    for p in params:
+        cache.host(2, p["N"], p["n_side"])
+    out = {"workload": f"{count} independent 2-D isentropic vortices on [0,10]^2, N~U{{3..8}}, "
+                       f"n_side~U{{4..48}}, beta~U(1,5), centre~U([2,8]^2), PCG64(seed+i), dt=0.002, "
+                       f"{steps} steps each", "instances": count, "steps": steps,
+           "host_mesh_setup_s": round(time.time() - t0, 2)}
+    finals = {}
+    for prec in (64, 32):
+        ens = B.VortexEnsemble(params, prec, nsteps=steps, cache=cache)
+        torch.cuda.synchronize()
+        ens.run(1)  # builds the step graph
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        ens.run(steps - 1)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        st = ens.batch.status()
+        finals[prec] = ens.results()
+        out[f"fp{prec}"] = {"value": ens.dof * 5 * (steps - 1) / (ms * 1e-3), "unit": METRIC,
+                            "ms_per_step": ms / (steps - 1), "dof": ens.dof,
+                            "solves_per_s": count / (ms * 1e-3 * steps / (steps - 1)),
+                            "state_finite": not bool(st.any()),
+                            "variants": {f"{d},{n}": v for (d, n), v in ens.variants().items()}}
+        ens.close()
+    err = np.zeros(4)
+    for a, b in zip(finals[32], finals[64]):
+        for q in range(4):
+            err[q] = max(err[q], np.linalg.norm(a[:, q] - b[:, q]) / np.linalg.norm(b[:, q]))
+    out["fp32_rel_l2_vs_fp64_max_over_instances"] = {"U": err[0], "V": err[1], "rho": err[2], "E": err[3]}
+    cache.close()
+    return out
+
+
 def dist_init():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     if ws <= 1:
@@ -230,6 +276,9 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the batched-ensemble measurement (run on 1 GPU only)")
+    ap.add_argument("--batched-instances", type=int, default=512)
     args = ap.parse_args()
 
     rank, world, local, tdist = dist_init()
@@ -334,6 +383,11 @@ def main():
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_sample(N, args.cpu_seconds)
+    if world == 1 and not args.no_batched:
+        bat = batched_ensemble(args.batched_instances, device=dev)
+        if args.precision == 64:
+            bat["fp32_over_fp64_plain"] = bat["fp32"]["value"] / value
+        line["batched"] = bat
     if rank == 0:
         print(json.dumps(line), flush=True)
     if tdist is not None:

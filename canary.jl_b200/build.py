@@ -53,9 +53,15 @@ def _stale(obj: str, src: str) -> bool:
     return any(os.path.getmtime(d) > t for d in [src] + _deps())
 
 
+# per-file flags: the geometry follows the reference's arithmetic without
+# multiply-add contraction
+FILE_FLAGS = {"cb_geometry.cu": ["-fmad=false"]}
+
+
 def _compile(src: str, verbose: bool) -> tuple[str, str]:
     obj = os.path.join(BUILD, os.path.basename(src)[:-3] + ".o")
-    cmd = [nvcc()] + NVCC_FLAGS + (["-Xptxas", "-v"] if verbose else []) + ["-c", src, "-o", obj]
+    extra = FILE_FLAGS.get(os.path.basename(src), [])
+    cmd = [nvcc()] + NVCC_FLAGS + extra + (["-Xptxas", "-v"] if verbose else []) + ["-c", src, "-o", obj]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"nvcc failed for {src}:\n{r.stdout}\n{r.stderr}")

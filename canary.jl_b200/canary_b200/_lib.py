@@ -25,7 +25,7 @@ EXPORTS = (
     "cb_volume_grad", "cb_flux_grad", "cb_update_gradQ", "cb_volume_div", "cb_flux_div",
     "cb_solver_create", "cb_lsrk_run", "cb_solver_set_offset", "cb_solver_sums",
     "cb_solver_destroy", "cb_lsrk_stage_noalloc",
-    "cb_mesh_create", "cb_mesh_destroy", "cb_batch_create", "cb_batch_set_variant", "cb_batch_add",
+    "cb_computegeometry", "cb_mesh_create", "cb_mesh_destroy", "cb_batch_create", "cb_batch_set_variant", "cb_batch_get_variant", "cb_batch_add",
     "cb_batch_run", "cb_batch_info", "cb_batch_release", "cb_batch_status", "cb_batch_destroy",
 )
 
@@ -81,10 +81,12 @@ def lib() -> C.CDLL:
     L.cb_solver_destroy.argtypes = [vp]
     L.cb_lsrk_stage_noalloc.argtypes = [C.c_int, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp, i64,
                                         phys_p, dbl, dbl, dbl, vp, vp]
+    L.cb_computegeometry.argtypes = [C.c_int, C.c_int, i64, vp, dbl, vp, vp, vp, vp, vp, vp]
     L.cb_mesh_create.argtypes = [C.POINTER(vp), C.c_int, C.c_int, C.c_int, i64, vp, vp, vp, vp, vp, vp, vp]
     L.cb_mesh_destroy.argtypes = [vp]
     L.cb_batch_create.argtypes = [C.POINTER(vp), C.c_int, C.c_int, phys_p, vp]
     L.cb_batch_set_variant.argtypes = [vp, C.c_int, C.c_int, C.c_int]
+    L.cb_batch_get_variant.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_int)]
     L.cb_batch_add.argtypes = [vp, vp, vp, vp, dbl, i64, C.POINTER(C.c_double), C.POINTER(C.c_int)]
     L.cb_batch_run.argtypes = [vp, i64]
     L.cb_batch_info.argtypes = [vp, C.c_int, C.POINTER(i64), C.POINTER(i64)]

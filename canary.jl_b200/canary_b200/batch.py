@@ -72,6 +72,12 @@ class Batch:
                                          _stream(stream)))
         self._inst = {}  # slot -> (mesh, Q, rhs, offset)
 
+    def variant(self, dim: int, N: int) -> int:
+        """Stage variant used for instances of (dim, N) admitted from now on."""
+        v = C.c_int(-1)
+        check(_lib.lib().cb_batch_get_variant(self._h, dim, N, C.byref(v)))
+        return v.value
+
     def set_variant(self, dim: int, N: int, variant: int) -> None:
         """Stage variant for instances of (dim, N) admitted from now on
         (VARIANTS); raises CanaryError for a variant not built for it."""
@@ -220,6 +226,10 @@ class VortexEnsemble:
     @property
     def dof(self) -> int:
         return 4 * self.nodes
+
+    def variants(self) -> dict:
+        """Stage variant used per (dim, N) present."""
+        return {(2, p["N"]): self.batch.variant(2, p["N"]) for p in self.params}
 
     def run(self, nsteps=None) -> None:
         self.batch.run(self.nsteps if nsteps is None else nsteps)

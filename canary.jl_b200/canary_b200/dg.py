@@ -253,6 +253,10 @@ def to_device(a: np.ndarray, dtype=None, device="cuda"):
     return t.to(device)
 
 
+def dev_i64(a, device="cuda"):
+    return to_device(a, _torch().int64, device)
+
+
 def from_device(t, shape) -> np.ndarray:
     """Flat tensor -> Fortran-ordered numpy array of the Julia shape."""
     return np.asarray(t.detach().cpu().numpy()).reshape(shape, order="F")
@@ -268,6 +272,44 @@ class DeviceMesh:
     vmapP: object
     elemtobndy: object
     D: object
+
+    @classmethod
+    def build(cls, dim, N, x, periodic, warp_amp=0.0, device="cuda", boundary=None, stream=None):
+        """Connectivity on the host (brickmesh -> partition -> connectmesh ->
+        mappings, euler3d_set3c.jl:1689-1708) and the grid and geometry on the
+        device in FP64 (cb_computegeometry), with the optional warp
+        x_c += warp_amp * prod_d sin(x_d).  The returned mesh has no host
+        copies of vgeo / sgeo (mesh.vgeo / mesh.sgeo are None)."""
+        torch = _torch()
+        from .operators import lglpoints, spectralderivative
+        cm = connectmesh(*partition(*brickmesh(x, periodic, boundary=boundary)))
+        vmapM, vmapP = mappings(N, cm["elemtoelem"], cm["elemtoface"], cm["elemtoordr"])
+        r, w = lglpoints(N)
+        D = spectralderivative(r)
+        e2c = np.asarray(cm["elemtocoord"], dtype=np.float64)
+        nelem = e2c.shape[2]
+        Nq = N + 1
+        Np, Nfp = Nq ** dim, Nq ** (dim - 1)
+        nvg, nsg = (14, 5) if dim == 3 else (8, 4)
+        dev = lambda a: to_device(a, torch.float64, device)
+        de2c, dr, dw, dD = dev(e2c), dev(np.asarray(r)), dev(np.asarray(w)), dev(D)
+        vgeo = torch.empty(Np * nvg * nelem, dtype=torch.float64, device=device)
+        sgeo = torch.empty(nsg * Nfp * 2 * dim * nelem, dtype=torch.float64, device=device)
+        check(_lib.lib().cb_computegeometry(dim, N, nelem, _ptr(de2c, torch.float64), float(warp_amp),
+                                            _ptr(dr, torch.float64), _ptr(dw, torch.float64),
+                                            _ptr(dD, torch.float64), _ptr(vgeo, torch.float64),
+                                            _ptr(sgeo, torch.float64), _stream(stream)))
+        mesh = Mesh(dim, N, nelem, None, None, vmapM, vmapP, cm["elemtobndy"], D, np.asarray(r),
+                    np.asarray(w), e2c)
+        return cls(mesh, vgeo, sgeo, dev_i64(vmapM, device), dev_i64(vmapP, device),
+                   dev_i64(cm["elemtobndy"], device), dD)
+
+    def coords(self):
+        """Node coordinates as device tensors (nelem, Np), one per dimension."""
+        m = self.mesh
+        nvg = 14 if m.dim == 3 else 8
+        v = self.vgeo.view(m.nelem, nvg, m.Np)
+        return tuple(v[:, m.dim * m.dim + 2 + c, :] for c in range(m.dim))
 
     @classmethod
     def upload(cls, mesh: Mesh, device="cuda"):

@@ -135,3 +135,61 @@ def vortex_ensemble(count: int = 512, seed: int = 0):
         xc, yc = (float(v) for v in rng.uniform(2.0, 8.0, 2))
         out.append(dict(N=N, n_side=n_side, beta=beta, xc=xc, yc=yc))
     return out
+
+
+# ----------------------------------------------------------- device forms
+def isentropic_vortex_t(x, y, beta=5.0, xc=5.0, yc=5.0, gamma=GAMMA):
+    """Torch form of isentropic_vortex at t = 0 for device tensors x, y;
+    returns (U, V, ρ, E) tensors."""
+    import torch
+    dx, dy = x - xc, y - yc
+    r2 = dx * dx + dy * dy
+    g1 = gamma - 1.0
+    dT = (-g1 * beta * beta / (8.0 * gamma * math.pi ** 2)) * torch.exp(1.0 - r2)
+    f = (beta / (2.0 * math.pi)) * torch.exp((1.0 - r2) / 2.0)
+    u = 1.0 - f * dy
+    v = f * dx
+    rho = (1.0 + dT) ** (1.0 / g1)
+    p = rho ** gamma
+    E = p / g1 + 0.5 * rho * (u * u + v * v)
+    return rho * u, rho * v, rho, E
+
+
+_FOURIER = {}
+
+
+def fourier_state_t(x, y, z, seed=0, kmax=4, gamma=GAMMA):
+    """Torch form of fourier_state for device tensors x, y, z (FP64), summing
+    16 wave vectors per batch; returns (U, V, W, ρ, E) tensors."""
+    import torch
+    key = (seed, kmax, str(x.device))
+    if key not in _FOURIER:
+        ks, coef = fourier_coefficients(seed, kmax)
+        K = torch.as_tensor(ks, dtype=torch.float64, device=x.device)
+        C = [(torch.as_tensor(a, dtype=torch.float64, device=x.device),
+              torch.as_tensor(phi, dtype=torch.float64, device=x.device)) for a, phi in coef]
+        _FOURIER[key] = (K, C)
+    K, C = _FOURIER[key]
+    X = [c.reshape(-1) for c in (x, y, z)]
+    out = []
+    for A, PH in C:
+        acc = torch.zeros_like(X[0])
+        for q0 in range(0, K.shape[0], 16):
+            sl = slice(q0, min(q0 + 16, K.shape[0]))
+            arg = (K[sl, 0:1] * X[0] + K[sl, 1:2] * X[1]) + K[sl, 2:3] * X[2] + PH[sl, None]
+            acc = acc + (A[sl, None] * torch.sin(arg)).sum(0)
+        out.append(acc.reshape(x.shape))
+    rho = 1.0 + out[0]
+    u, v, w = out[1], out[2], out[3]
+    E = 1.0 / (gamma - 1.0) + 0.5 * rho * (u * u + v * v + w * w)
+    return rho * u, rho * v, rho * w, rho, E
+
+
+def device_state(fields, dtype=None, offset=None):
+    """Pack per-field device tensors (nelem, Np) into the flat (Np, nstate,
+    nelem) column-major state, minus the per-field `offset`, cast to dtype."""
+    import torch
+    Q = torch.stack(fields, dim=1)  # (nelem, nstate, Np) C order == (Np, nstate, nelem) F order
+    if offset is not None:
+        Q = Q - torch.as_tensor(offset, dtype=Q.dtype, device=Q.device).view(1, -1, 1)
+    return Q.to(dtype or Q.dtype).contiguous().reshape(-1)

@@ -183,6 +183,26 @@ int cb_solver_sums(cb_solver *s, double *out_host);
 int cb_solver_destroy(cb_solver *s);
 
 /* ---------------------------------------------------------------------- */
+/* Device-side geometry.                                                   */
+/* ---------------------------------------------------------------------- */
+
+/* vgeo and sgeo of an element mesh computed on the device in FP64: the LGL
+ * grid blended from the element corners (creategrid, metric.jl:11-107), the
+ * optional warp x_c += warp_amp * prod_d sin(x_d) (0: none), the metric terms
+ * (computemetric, metric.jl:155-208 in 2-D and the curl-invariant form of
+ * metric.jl:230-400 in 3-D) and computegeometry's vgeo / sgeo assembly
+ * (euler3d_set3c.jl:210-248).  Replaces the host setup of those arrays.
+ * elemtocoord is (dim, 2^dim, nelem); r, w the LGL points and weights (Nq);
+ * D the derivative matrix; all device pointers.  sgeo's vMJI entry is MJI at
+ * the face node of the element itself (vmapM of a conforming mesh).  The sums
+ * follow the reference's order without multiply-add contraction; results
+ * agree with a host evaluation to the last bits of sin and hypot. */
+int cb_computegeometry(int dim, int N, int64_t nelem, const double *elemtocoord,
+                       double warp_amp, const double *r, const double *w,
+                       const double *D, double *vgeo, double *sgeo,
+                       cb_stream_t stream);
+
+/* ---------------------------------------------------------------------- */
 /* Batched LSRK(5,4) over many independent instances (ensembles, serving). */
 /* ---------------------------------------------------------------------- */
 
@@ -212,11 +232,16 @@ int cb_mesh_destroy(cb_mesh *m);
 typedef struct cb_batch cb_batch;
 int cb_batch_create(cb_batch **out, int precision, int max_instances,
                     const cb_phys *phys, cb_stream_t stream);
-/* Element-group shape used for instances of (dim, N) admitted from now on:
- * variant 0 groups about 256 nodes per block, variant 1 about 512
- * (CB_ERR_UNSUPPORTED where it would need more than two nodes per thread).
- * Chosen by an autotuner; the results do not depend on it. */
+/* Stage variant used for instances of (dim, N) admitted from now on:
+ * 0 = pipelined bulk-copy staging at its default occupancy (where every slab
+ * is a multiple of 16 bytes: all 2-D orders, 3-D odd orders), 1 / 2 = grouped
+ * staging with about 256 / 512 nodes per block, 3 / 4 = pipelined staging
+ * compiled for the other occupancies (2, 3 or 4 blocks per SM).  Variants
+ * that are not built for (dim, N) give CB_ERR_UNSUPPORTED.  Chosen by an
+ * autotuner; the pipelined variants agree bit for bit among themselves, as do
+ * the grouped ones, and the two families to round-off. */
 int cb_batch_set_variant(cb_batch *b, int dim, int N, int variant);
+int cb_batch_get_variant(const cb_batch *b, int dim, int N, int *variant);
 /* Admit an instance: the caller's state Q and zeroed residual carry rhs
  * (layouts as above, precision of the batch) advance by nsteps steps of dt
  * during the following cb_batch_run calls.  qref (nstate doubles, or NULL for

@@ -1,0 +1,39 @@
+"""Host side of the serving loop (no GPU): the request stream and the time
+step plan."""
+import math
+
+import numpy as np
+
+from canary_b200 import serve as S
+
+
+def test_request_stream_is_seeded_and_follows_the_mix():
+    a = S.request_stream(2000, rate=50.0, seed=7)
+    b = S.request_stream(2000, rate=50.0, seed=7)
+    assert [(r.kind, r.N, r.n_side, r.t_final, r.arrival) for r in a] == \
+           [(r.kind, r.N, r.n_side, r.t_final, r.arrival) for r in b]
+    kinds = np.array([r.kind for r in a])
+    assert abs(np.mean(kinds == "vortex") - 0.70) < 0.04
+    assert abs(np.mean(kinds != "vortex") - 0.30) < 0.04
+    for r in a:
+        if r.kind == "vortex":
+            assert 3 <= r.N <= 8 and 8 <= r.n_side <= 64 and 1 <= r.beta <= 5
+            assert 2 <= r.xc <= 8 and 2 <= r.yc <= 8
+        else:
+            assert 3 <= r.N <= 7 and 4 <= r.n_side <= 16
+        assert 0.5 <= r.t_final <= 2.0
+    arr = np.array([r.arrival for r in a])
+    assert np.all(np.diff(arr) >= 0)
+    gaps = np.diff(arr)
+    assert abs(gaps.mean() - 1 / 50.0) < 0.1 / 50.0  # Poisson rate 50/s
+    assert all(r.arrival == 0.0 for r in S.request_stream(10, rate=0.0))
+
+
+def test_plan_reaches_the_final_time():
+    r = S.Request(0, "vortex", 8, 64, 1.3, 0.0)
+    n, dt = S.plan(r, 2.9)
+    assert abs(n * dt - 1.3) < 1e-12
+    assert dt <= 0.2 * (10.0 / 64) / (64 * 2.9) + 1e-15
+    r3 = S.Request(1, "euler3d", 7, 16, 0.5, 0.0)
+    n3, dt3 = S.plan(r3, 1.3)
+    assert n3 == math.ceil(0.5 / (0.2 * (2 * math.pi / 16) / (49 * 1.3)))
