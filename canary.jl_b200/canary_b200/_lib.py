@@ -24,9 +24,9 @@ EXPORTS = (
     "cb_updatesolution", "cb_updatesolution_f32",
     "cb_volume_grad", "cb_flux_grad", "cb_update_gradQ", "cb_volume_div", "cb_flux_div",
     "cb_solver_create", "cb_lsrk_run", "cb_solver_set_offset", "cb_solver_sums",
-    "cb_solver_destroy", "cb_lsrk_stage_noalloc",
+    "cb_solver_destroy", "cb_solver_status_async", "cb_lsrk_stage_noalloc",
     "cb_computegeometry", "cb_mesh_create", "cb_mesh_destroy", "cb_batch_create", "cb_batch_set_variant", "cb_batch_get_variant", "cb_batch_add",
-    "cb_batch_run", "cb_batch_info", "cb_batch_release", "cb_batch_status", "cb_batch_destroy",
+    "cb_batch_run", "cb_batch_info", "cb_batch_release", "cb_batch_status", "cb_batch_status_async", "cb_batch_destroy",
 )
 
 
@@ -93,6 +93,8 @@ def lib() -> C.CDLL:
     L.cb_batch_release.argtypes = [vp, C.c_int]
     L.cb_batch_status.argtypes = [vp, C.POINTER(C.c_uint)]
     L.cb_batch_destroy.argtypes = [vp]
+    L.cb_batch_status_async.argtypes = [vp, vp]
+    L.cb_solver_status_async.argtypes = [vp, vp]
     _lib = L
     return L
 

@@ -143,6 +143,11 @@ class Batch:
         check(_lib.lib().cb_batch_status(self._h, out))
         return np.array(out[:], dtype=np.uint32)
 
+    def status_async(self, host) -> None:
+        """Enqueue a copy of the per-slot status bits into `host` (a pinned
+        int32 tensor of max_instances entries) on the batch stream."""
+        check(_lib.lib().cb_batch_status_async(self._h, C.c_void_p(host.data_ptr())))
+
     def close(self) -> None:
         if self._h:
             _lib.lib().cb_batch_destroy(self._h)

@@ -380,6 +380,11 @@ class LSRK:
     def run(self, nsteps: int, dt: float) -> None:
         check(_lib.lib().cb_lsrk_run(self._h, int(nsteps), float(dt)))
 
+    def status_async(self, host) -> None:
+        """Enqueue a copy of the status bits into `host` (a pinned int32
+        tensor) on the solver's stream."""
+        check(_lib.lib().cb_solver_status_async(self._h, C.c_void_p(host.data_ptr())))
+
     def sums(self) -> np.ndarray:
         """Compensated FP64 (Σ MJ Q_s, Σ MJ Q_s²) per field, shape (2, nstate)."""
         ns = nstate(self.dmesh.mesh.dim)

@@ -554,6 +554,13 @@ int cb_batch_set_variant(cb_batch *b, int dim, int N, int variant) {
   return CB_OK;
 }
 
+int cb_batch_get_variant(const cb_batch *b, int dim, int N, int *variant) {
+  if (!b || !variant || (dim != 2 && dim != 3) || !b_order_ok(dim, N))
+    return solver_fail(CB_ERR_ARG, "cb_batch_get_variant: bad arguments");
+  *variant = b->var[dim - 2][N];
+  return CB_OK;
+}
+
 int cb_batch_add(cb_batch *b, const cb_mesh *m, void *Q, void *rhs, double dt, int64_t nsteps, const double *qref,
                  int *slot) {
   if (!b || !m || !Q || !rhs || !slot || nsteps < 0 || !std::isfinite(dt))
@@ -591,6 +598,13 @@ int cb_batch_status(cb_batch *b, unsigned *out_host) {
       (e = cudaStreamSynchronize(b->stream)) != cudaSuccess)
     return solver_fail(CB_ERR_CUDA, "cb_batch_status: %s", cudaGetErrorString(e));
   return CB_OK;
+}
+
+int cb_batch_status_async(cb_batch *b, unsigned *out_host) {
+  if (!b || !out_host) return solver_fail(CB_ERR_ARG, "cb_batch_status_async: null argument");
+  const cudaError_t e =
+      cudaMemcpyAsync(out_host, b->status, sizeof(unsigned) * b->cap, cudaMemcpyDeviceToHost, b->stream);
+  return e == cudaSuccess ? CB_OK : solver_fail(CB_ERR_CUDA, "cb_batch_status_async: %s", cudaGetErrorString(e));
 }
 
 int cb_batch_destroy(cb_batch *b) {

@@ -299,6 +299,12 @@ int cb_solver_set_offset(cb_solver *s, const double *qref) {
   return CB_OK;
 }
 
+int cb_solver_status_async(cb_solver *s, unsigned *out_host) {
+  if (!s || !out_host) return solver_fail(CB_ERR_ARG, "cb_solver_status_async: null argument");
+  const cudaError_t e = cudaMemcpyAsync(out_host, s->status, sizeof(unsigned), cudaMemcpyDeviceToHost, s->stream);
+  return e == cudaSuccess ? CB_OK : solver_fail(CB_ERR_CUDA, "cb_solver_status_async: %s", cudaGetErrorString(e));
+}
+
 int cb_solver_destroy(cb_solver *s) {
   if (!s) return CB_OK;
   if (s->stream) cudaStreamSynchronize(s->stream);

@@ -180,6 +180,10 @@ int cb_solver_set_offset(cb_solver *s, const double *qref);
 /* Compensated (Neumaier) FP64 sums over all nodes of MJ·Q[:,s,:] and
  * MJ·Q[:,s,:]² for every state field s: out[2*nstate]; synchronises. */
 int cb_solver_sums(cb_solver *s, double *out_host);
+/* Enqueue on the solver's stream a copy of its status bits (bit 2:
+ * non-finite state) into *out_host (page-locked memory for an asynchronous
+ * copy); the value is valid once the stream has reached the copy. */
+int cb_solver_status_async(cb_solver *s, unsigned *out_host);
 int cb_solver_destroy(cb_solver *s);
 
 /* ---------------------------------------------------------------------- */
@@ -262,6 +266,9 @@ int cb_batch_release(cb_batch *b, int slot);
 /* Per-slot sticky status bits (out_host[max_instances]; bit 2 = non-finite
  * state); synchronises. */
 int cb_batch_status(cb_batch *b, unsigned *out_host);
+/* The same copy enqueued on the batch stream without synchronising (for a
+ * serving loop that polls an event after it). */
+int cb_batch_status_async(cb_batch *b, unsigned *out_host);
 int cb_batch_destroy(cb_batch *b);
 
 /* ---------------------------------------------------------------------- */
