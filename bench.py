@@ -133,6 +133,24 @@ def setup_workload(n_side, N, device="cuda", seed=0):
     return mesh, Q, dt
 
 
+def setup_device_workload(n_side, N, precision, device="cuda", seed=0):
+    """The same workload built on the device: connectivity on the host, grid,
+    warp and geometry by cb_computegeometry, the Fourier state by torch.
+    Returns (DeviceMesh, Q, rhs, dt, offset) with Q, rhs in the working
+    precision (for FP32 Q holds the state minus its per-field mean)."""
+    import torch
+    from canary_b200 import dg, ic, serve
+    L = 2 * math.pi
+    x = (np.linspace(0.0, L, n_side + 1),) * 3
+    dm = dg.DeviceMesh.build(3, N, x, (True,) * 3, warp_amp=0.05, device=device)
+    f = ic.fourier_state_t(*dm.coords(), seed=seed)
+    dt = 0.2 * (L / n_side) / (N * N * float(serve.wave_speed(f, 3).item()))
+    off = np.array([float(t.mean().item()) for t in f]) if precision == 32 else np.zeros(5)
+    real = torch.float64 if precision == 64 else torch.float32
+    Q = ic.device_state(list(f), real, off)
+    return dm, Q, torch.zeros_like(Q), dt, off
+
+
 def cpu_sample(N, seconds=10.0, n_side=16, max_steps=40):
     """Oracle (CPU restatement of the reference's CPU path) on a bounded
     sample of the workload: same N, warp and initial-state law on an
@@ -279,6 +297,10 @@ def main():
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched-ensemble measurement (run on 1 GPU only)")
     ap.add_argument("--batched-instances", type=int, default=512)
+    ap.add_argument("--no-served", action="store_true",
+                    help="skip the served-stream measurement (run on 1 GPU only)")
+    ap.add_argument("--served-requests", type=int, default=150)
+    ap.add_argument("--served-baseline", type=int, default=30)
     args = ap.parse_args()
 
     rank, world, local, tdist = dist_init()
@@ -295,11 +317,11 @@ def main():
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
     N, dim = args.order, 3
-    mesh, Q, dt = setup_workload(args.n_side, N, device=dev)
-    dm = dg.DeviceMesh.upload(mesh, device=dev)
+    dm, dQ, drhs, dt, off = setup_device_workload(args.n_side, N, args.precision, device=dev)
+    mesh = dm.mesh
     real = torch.float64 if args.precision == 64 else torch.float32
-    solver = dg.LSRK.for_state(dm, Q, args.precision, dg.make_phys(), stream)
-    dQ, drhs = solver.Q, solver.rhs
+    solver = dg.LSRK(dm, dQ, drhs, args.precision, dg.make_phys(), stream)
+    solver.set_offset(off)
     dof = mesh.nelem * mesh.Np * 5
 
     solver.run(args.warmup, dt)
@@ -388,6 +410,10 @@ def main():
         if args.precision == 64:
             bat["fp32_over_fp64_plain"] = bat["fp32"]["value"] / value
         line["batched"] = bat
+    if world == 1 and not args.no_served:
+        from canary_b200 import serve
+        line["served"] = serve.benchmark(args.served_requests, seed=0, precision=32,
+                                         baseline_count=args.served_baseline, device=str(dev))
     if rank == 0:
         print(json.dumps(line), flush=True)
     if tdist is not None:

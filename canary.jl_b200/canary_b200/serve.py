@@ -53,15 +53,17 @@ class Request:
 
 def request_stream(count: int, rate: float, seed: int = 0, mix=(0.70, 0.15, 0.15)):
     """`count` requests with Poisson arrivals of rate `rate` per second (all
-    at t = 0 when rate <= 0), drawn from numpy's PCG64(seed): kind by `mix`
-    (vortex, 3-D Euler, 3-D Navier–Stokes); vortex N ~ U{3..8}, n_side ~
-    U{8..64}, beta ~ U(1,5), centre ~ U([2,8]^2); 3-D N ~ U{3..7}, n_side ~
-    U{4..16}, Fourier seed = request id; t_final ~ U(0.5, 2)."""
+    at t = 0 when rate <= 0).  Parameters are drawn from numpy's PCG64(seed)
+    (the same requests at every rate), arrival gaps from PCG64(seed + 2^32):
+    kind by `mix` (vortex, 3-D Euler, 3-D Navier–Stokes); vortex N ~ U{3..8},
+    n_side ~ U{8..64}, beta ~ U(1,5), centre ~ U([2,8]^2); 3-D N ~ U{3..7},
+    n_side ~ U{4..16}, Fourier seed = request id; t_final ~ U(0.5, 2)."""
     rng = np.random.Generator(np.random.PCG64(seed))
+    arr = np.random.Generator(np.random.PCG64(seed + 2 ** 32))
     t, out = 0.0, []
     for i in range(count):
         if rate > 0:
-            t += float(rng.exponential(1.0 / rate))
+            t += float(arr.exponential(1.0 / rate))
         u = float(rng.random())
         kind = "vortex" if u < mix[0] else ("euler3d" if u < mix[0] + mix[1] else "ns3d")
         if kind == "vortex":
@@ -161,6 +163,10 @@ class _Live:
     stream: object = None
     left: int = 0
     admitted: float = 0.0
+    failed: bool = False
+    tick0: int = 0  # loop tick at admission
+    stat: object = None  # pinned status word (viscous solver)
+    stat_ev: object = None
 
 
 @dataclass
@@ -210,7 +216,8 @@ class Server:
     state offsets); tick_steps steps are launched per loop iteration, with at
     most two ticks in flight."""
 
-    def __init__(self, precision=32, hbm_budget=120e9, max_instances=4096, tick_steps=8, device="cuda"):
+    def __init__(self, precision=32, hbm_budget=120e9, max_instances=4096, tick_steps=8, device="cuda",
+                 viscous_streams=8):
         torch = _torch()
         self.torch = torch
         self.device = torch.device(device)
@@ -220,8 +227,11 @@ class Server:
         self.tick = tick_steps
         self.bstream = torch.cuda.Stream(self.device)  # batch and its admissions / retirements
         self.sstream = torch.cuda.Stream(self.device)  # meshes and initial states
-        self.vstream = torch.cuda.Stream(self.device)  # viscous requests
+        # viscous requests: one solver each, spread over a few streams so that
+        # small solves run concurrently
+        self.vstreams = [torch.cuda.Stream(self.device) for _ in range(viscous_streams)]
         self.batch = Batch(precision, max_instances, make_phys(), stream=self.bstream)
+        self.max_instances = max_instances
         self.vphys = make_phys(visc=VISC)
         self.pool = MeshPool(self.device, self.sstream)
         self.in_use = 0
@@ -258,11 +268,13 @@ class Server:
         nsteps, dt = plan(req, speed)
         live = _Live(req, m, nsteps, dt, self.request_bytes(req), off, Q, rhs, left=nsteps, admitted=now)
         if req.kind == "ns3d":
-            live.stream = self.vstream
-            self.vstream.wait_stream(self.sstream)
-            Q.record_stream(self.vstream)
-            rhs.record_stream(self.vstream)
-            live.solver = LSRK(m.dmesh, Q, rhs, self.precision, self.vphys, stream=self.vstream)
+            vs = self.vstreams[req.rid % len(self.vstreams)]
+            live.stream = vs
+            vs.wait_stream(self.sstream)
+            Q.record_stream(vs)
+            rhs.record_stream(vs)
+            live.solver = LSRK(m.dmesh, Q, rhs, self.precision, self.vphys, stream=vs)
+            live.stat = torch.zeros(1, dtype=torch.int32, pin_memory=True)
         else:
             self.bstream.wait_stream(self.sstream)
             Q.record_stream(self.bstream)
@@ -285,12 +297,23 @@ class Server:
         reqs = deque(sorted(requests, key=lambda r: (r.arrival, r.rid)))
         waiting, live, retiring = deque(), {}, []
         lat, results, failed = {}, {}, set()
-        flight = deque()
+        flight = {}  # stream -> events of the ticks in flight
+        bstat = torch.zeros(self.max_instances, dtype=torch.int32, pin_memory=True)
+        bstat_ev, bstat_tick, ticks = None, 0, 0
         dof_stage, peak, max_live = 0.0, 0, 0
         base = torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize(self.device)
         base.record(self.bstream)
         t0 = time.perf_counter()
+
+        def tick_done(stream):
+            ev = torch.cuda.Event()
+            ev.record(stream)
+            q = flight.setdefault(stream, deque())
+            q.append(ev)
+            if len(q) > 2:  # at most two ticks in flight per stream
+                q.popleft().synchronize()
+
         while reqs or waiting or live or retiring:
             now = time.perf_counter() - t0
             while reqs and (not realtime or reqs[0].arrival <= now):
@@ -298,14 +321,29 @@ class Server:
             while waiting and self._fits(waiting[0]):
                 r = waiting.popleft()
                 lv = self.admit(r, time.perf_counter() - t0)
+                lv.tick0 = ticks
                 live[r.rid] = lv
             if waiting and not live and not retiring and not self._fits(waiting[0]):
                 raise RuntimeError(f"request {waiting[0].rid} does not fit the HBM budget on its own")
             peak = max(peak, self.in_use + self.pool.resident_bytes())
             max_live = max(max_live, len(live))
+            # non-finite states (status copied after an earlier tick): retire early as failed
+            if bstat_ev is not None and bstat_ev.query():
+                bits = bstat.numpy()
+                for lv in live.values():
+                    # a slot's word is reset at admission: only instances admitted
+                    # before the copied tick are described by it
+                    if lv.solver is None and lv.tick0 < bstat_tick and bits[lv.slot] & 2:
+                        lv.failed = True
+                bstat_ev = None
+            for lv in live.values():
+                if lv.solver is not None and lv.stat_ev is not None and lv.stat_ev.query():
+                    lv.failed = bool(int(lv.stat[0]) & 2)
+                    lv.stat_ev = None
             if live:
                 # one tick: K batch steps and K steps of every viscous solver
                 self.batch.run(self.tick)
+                used = set()
                 for rid, lv in list(live.items()):
                     Nq = lv.req.N + 1
                     dofs = nstate(lv.req.dim) * (lv.req.n_side ** lv.req.dim) * Nq ** lv.req.dim
@@ -313,21 +351,30 @@ class Server:
                         done, target = self.batch.info(lv.slot)
                         dof_stage += 5 * dofs * (lv.left - (target - done))
                         lv.left = target - done
-                    else:
+                    elif not lv.failed:
                         k = min(self.tick, lv.left)
                         lv.solver.run(k, lv.dt)
                         lv.left -= k
                         dof_stage += 5 * dofs * k
-                    if lv.left <= 0:
+                        used.add(lv.stream)
+                        if lv.stat_ev is None and lv.left > 0:
+                            lv.solver.status_async(lv.stat)
+                            lv.stat_ev = torch.cuda.Event()
+                            lv.stat_ev.record(lv.stream)
+                    if lv.left <= 0 or lv.failed:
+                        if lv.failed:
+                            failed.add(rid)
                         retiring.append(self._retire(lv))
                         del live[rid]
-                # the batch stream's tick event also covers the viscous tick
-                self.bstream.wait_stream(self.vstream)
-                ev = torch.cuda.Event()
-                ev.record(self.bstream)
-                flight.append(ev)
-                if len(flight) > 2:
-                    flight.popleft().synchronize()
+                ticks += 1
+                if bstat_ev is None:
+                    self.batch.status_async(bstat)
+                    bstat_ev = torch.cuda.Event()
+                    bstat_ev.record(self.bstream)
+                    bstat_tick = ticks
+                tick_done(self.bstream)
+                for vs in used:
+                    tick_done(vs)
             elif reqs and realtime:
                 time.sleep(max(0.0, min(reqs[0].arrival - (time.perf_counter() - t0), 0.002)))
             for item in list(retiring):
@@ -347,9 +394,6 @@ class Server:
             if not live and retiring:
                 retiring[0][0].synchronize()
         torch.cuda.synchronize(self.device)
-        end_ev = torch.cuda.Event(enable_timing=True)
-        end_ev.record(self.bstream)
-        end_ev.synchronize()
         arrival = {r.rid: (r.arrival if realtime else 0.0) for r in requests}
         first = min(arrival.values())
         last = max(lat[k] + arrival[k] for k in lat)
@@ -386,7 +430,7 @@ def serve_one_at_a_time(requests, precision=64, device="cuda"):
     dev = torch.device(device)
     stream = torch.cuda.Stream(dev)
     pool = MeshPool(dev, stream)
-    lat, results = {}, {}
+    lat, results, failed = {}, {}, set()
     dof_stage = 0.0
     real = torch.float64 if precision == 64 else torch.float32
     base = torch.cuda.Event(enable_timing=True)
@@ -419,6 +463,8 @@ def serve_one_at_a_time(requests, precision=64, device="cuda"):
         s.close()
         lat[r.rid] = base.elapsed_time(ev) * 1e-3 - r.arrival
         results[r.rid] = host.numpy().reshape((r.n_side ** r.dim, nstate(r.dim), (r.N + 1) ** r.dim)).transpose(2, 1, 0)
+        if not np.all(np.isfinite(results[r.rid])):
+            failed.add(r.rid)
         dof_stage += 5 * nstate(r.dim) * (r.n_side ** r.dim) * (r.N + 1) ** r.dim * nsteps
         pool.release(r)
     first = min(r.arrival for r in requests)
@@ -426,4 +472,53 @@ def serve_one_at_a_time(requests, precision=64, device="cuda"):
     for m in pool.meshes.values():
         for bm in m.batch.values():
             bm.close()
-    return Report(lat, results, first, last, dof_stage, 0, 1)
+    return Report(lat, results, first, last, dof_stage, 0, 1, failed)
+
+
+def benchmark(count=2000, seed=0, precision=32, hbm_budget=120e9, tick_steps=8, load=0.8,
+              baseline_count=100, device="cuda"):
+    """The served stream: (1) capacity = solves/s of the closed loop with all
+    `count` requests present at t = 0; (2) the same requests arriving as a
+    Poisson stream at `load` x capacity, served in real time (p50/p99 latency,
+    solves/s); (3) the first `baseline_count` of them one at a time through
+    the plain FP64 path, and the same subset through the server, on the same
+    arrival times."""
+    cap_reqs = request_stream(count, 0.0, seed)
+    srv = Server(precision, hbm_budget, tick_steps=tick_steps, device=device)
+    cap = srv.serve(cap_reqs, realtime=False).summary()
+    srv.close()
+    rate = load * cap["solves_per_s"]
+    reqs = request_stream(count, rate, seed)
+    srv = Server(precision, hbm_budget, tick_steps=tick_steps, device=device)
+    served = srv.serve(reqs, realtime=True)
+    srv.close()
+    sub = reqs[:baseline_count]
+    srv = Server(precision, hbm_budget, tick_steps=tick_steps, device=device)
+    sub_served = srv.serve(sub, realtime=True).summary()
+    srv.close()
+    seq = serve_one_at_a_time(sub, 64, device).summary()
+    kinds = {k: sum(1 for r in reqs if r.kind == k) for k in KINDS}
+    return {"requests": count, "mix": kinds, "seed": seed, "precision": precision,
+            "hbm_budget_bytes": int(hbm_budget), "tick_steps": tick_steps,
+            "capacity": cap, "rate_per_s": rate, "load": load, "served": served.summary(),
+            "subset": {"requests": len(sub), "served": sub_served, "one_at_a_time_fp64": seq}}
+
+
+def main(argv=None):
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description="served stream of DG solve requests")
+    ap.add_argument("--requests", type=int, default=2000)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--precision", type=int, default=32, choices=[32, 64])
+    ap.add_argument("--budget-gb", type=float, default=120.0)
+    ap.add_argument("--tick", type=int, default=8)
+    ap.add_argument("--load", type=float, default=0.8)
+    ap.add_argument("--baseline", type=int, default=100)
+    a = ap.parse_args(argv)
+    out = benchmark(a.requests, a.seed, a.precision, a.budget_gb * 1e9, a.tick, a.load, a.baseline)
+    print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()
