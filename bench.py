@@ -76,17 +76,35 @@ class ClockSampler:
         self.uuid = uuid
         self.proc = None
         self.path = None
+        self.skip = 0
 
     def start(self):
         try:
             fd, self.path = tempfile.mkstemp(suffix=".csv")
             os.close(fd)
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200",
+                                          "--format=csv,noheader,nounits", "-lms", "50",
                                           "-f", self.path],
                                          stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+
+    def _lines(self):
+        try:
+            with open(self.path) as f:
+                return sum(1 for _ in f)
+        except Exception:
+            return 0
+
+    def mark(self):
+        """Wait (up to 3 s) until the sampler has written a first sample, then
+        remember how many were taken before the timed region."""
+        if self.proc is None:
+            return
+        t = time.time()
+        while self._lines() == 0 and time.time() - t < 3.0:
+            time.sleep(0.01)
+        self.skip = self._lines()
 
     def stop(self):
         if self.proc is None:
@@ -111,6 +129,9 @@ class ClockSampler:
             return None
         if not rows:
             return None
+        # samples taken during (and just after) the timed region; the last one
+        # if the region was shorter than the sampling interval
+        rows = rows[self.skip:] if len(rows) > self.skip else rows[-1:]
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
         mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
         names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
@@ -332,6 +353,7 @@ def main():
         uuid = None
     clocks = ClockSampler(uuid)
     clocks.start()
+    clocks.mark()
     if tdist is not None:
         tdist.barrier()
     torch.cuda.synchronize(dev)
