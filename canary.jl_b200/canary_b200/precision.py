@@ -11,6 +11,13 @@ with the seeded Fourier state, inviscid and with the LDG Navier–Stokes terms
 The FP64 form is itself pinned to the CPU oracle at 1e-12 on smaller meshes
 (tests/test_gpu_parity.py, tests/test_geometry.py).  Errors are relative L2
 norms per state field, evaluated on the device in FP64.
+
+The seeded Fourier state steepens into shocks, which the unlimited DG scheme
+(the reference's as well) does not survive: on the oracle it turns non-finite
+by t = 0.09-0.15 on 4^3-8^3 meshes.  The 3-D time step is therefore
+min(0.2 h / (N^2 max(|u|+c)), t_smooth / steps) with t_smooth = 0.08, so that
+the requested number of steps (the accumulation of FP32 rounding that the
+report measures) stays in the smooth regime.
 """
 from __future__ import annotations
 
@@ -29,7 +36,10 @@ def _rel_l2(a, b):
             for s in range(b.shape[1])]
 
 
-def run_case(dim, N, n_side, steps, visc=0.0, seed=0, device="cuda"):
+T_SMOOTH = 0.08
+
+
+def run_case(dim, N, n_side, steps, visc=0.0, seed=0, device="cuda", t_smooth=T_SMOOTH):
     torch = _torch()
     from .serve import wave_speed
     if dim == 3:
@@ -37,7 +47,7 @@ def run_case(dim, N, n_side, steps, visc=0.0, seed=0, device="cuda"):
         x = (np.linspace(0.0, L, n_side + 1),) * 3
         dm = DeviceMesh.build(3, N, x, (True,) * 3, warp_amp=0.05, device=device)
         f = ic.fourier_state_t(*dm.coords(), seed=seed)
-        dt = 0.2 * (L / n_side) / (N * N * float(wave_speed(f, 3).item()))
+        dt = min(0.2 * (L / n_side) / (N * N * float(wave_speed(f, 3).item())), t_smooth / steps)
     else:
         x = (np.linspace(0.0, 10.0, n_side + 1),) * 2
         dm = DeviceMesh.build(2, N, x, (True,) * 2, device=device)
