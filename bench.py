@@ -418,7 +418,7 @@ def main():
                    "state_finite": finite},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
-                     "traffic": traffic, "bytes_per_node": bpn, "kernel": "k_stage",
+                     "traffic": traffic, "bytes_per_node": bpn, "kernel": "k_stage_pipe2",
                      "launch_ms": t_launch * 1e3},
         "e2e": {"value": world * dof * 5 * args.e2e_steps / (e2e_ms * 1e-3), "unit": METRIC,
                 "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo, "steps": args.e2e_steps},
