@@ -207,3 +207,13 @@ def test_batch_matches_single_solver(cases):
     s.close()
     got = _run_batch(cases, 64, idx=[7], chunks=(100,))[0]
     assert max(relerr_fields(got, single)) < 1e-13
+
+
+def test_autotuner_picks_a_built_variant():
+    tuned = B.autotune(32, [(2, 3), (3, 4)], nodes_target=20000, steps=1, repeat=1)
+    b = B.Batch(32, 1)
+    for (dim, N), v in tuned.items():
+        b.set_variant(dim, N, v)  # raises if the chosen variant is not built
+        assert b.variant(dim, N) == v
+    b.close()
+    assert (3, 4) in tuned and tuned[(3, 4)] in (1, 2)  # 3-D even order: no pipelined variant
