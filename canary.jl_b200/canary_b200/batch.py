@@ -25,6 +25,7 @@ MAX_ORDER = {2: 8, 3: 7}  # orders compiled into the batched stage
 # SM (blocks of up to 256 threads)
 VARIANTS = (0, 1, 2, 3, 4)
 PIPELINED = (0, 3, 4)
+VAR_AFFINE = 5  # the pipelined stage with affine-element geometry (chosen by the batch)
 
 
 class BatchMesh:
@@ -46,6 +47,14 @@ class BatchMesh:
     @property
     def Np(self) -> int:
         return (self.N + 1) ** self.dim
+
+    @property
+    def affine(self) -> bool:
+        """Whether every element is affine (the batch then uses the
+        affine-element stage for it, see Batch.set_affine)."""
+        v = C.c_int(0)
+        check(_lib.lib().cb_mesh_affine(self._h, C.byref(v)))
+        return bool(v.value)
 
     def close(self) -> None:
         if self._h:
@@ -82,6 +91,13 @@ class Batch:
         """Stage variant for instances of (dim, N) admitted from now on
         (VARIANTS); raises CanaryError for a variant not built for it."""
         check(_lib.lib().cb_batch_set_variant(self._h, dim, N, variant))
+
+    def set_affine(self, on: bool) -> None:
+        """Whether instances admitted from now on use the affine-element stage
+        where it applies (affine mesh, gravity 0, pipelined variant; on by
+        default): it reads one geometry record per element instead of the
+        per-node metric and face geometry, and agrees with them to round-off."""
+        check(_lib.lib().cb_batch_set_affine(self._h, 1 if on else 0))
 
     def add(self, mesh: BatchMesh, Q, rhs, dt: float, nsteps: int, qref=None) -> int:
         """Admit the caller's device state Q and zeroed carry rhs (flat tensors
@@ -121,6 +137,13 @@ class Batch:
         done, target = C.c_int64(), C.c_int64()
         check(_lib.lib().cb_batch_info(self._h, slot, C.byref(done), C.byref(target)))
         return done.value, target.value
+
+    def slot_variant(self, slot: int) -> int:
+        """Stage variant the slot runs with (VAR_AFFINE: the affine-element
+        stage)."""
+        v = C.c_int(-1)
+        check(_lib.lib().cb_batch_slot_variant(self._h, slot, C.byref(v)))
+        return v.value
 
     def release(self, slot: int):
         """Retire a slot; its final state is placed in the caller's Q.

@@ -75,6 +75,98 @@ __global__ void k_batch_invalidate(BHdr *hdr, int sid, int pos, int n, int count
   for (int g = t; g < n; g += gridDim.x * blockDim.x) work[pos + g].valid = 0;
 }
 
+// LGL weights of order N (the Newton iteration on (1 - x^2) P_N'(x) = 0 from
+// the Chebyshev-Gauss-Lobatto points, G. von Winckel's lglnodes; w_i =
+// 2 / (N (N + 1) P_N(x_i)^2)), as GaussQuadrature.jl's lglpoints gives them
+// to round-off.
+void lgl_weights(int N, double *w) {
+  const double pi = 3.14159265358979323846;
+  for (int i = 0; i <= N; ++i) {
+    double x = std::cos(pi * i / N), PN = 1.0;
+    for (int it = 0; it < 100; ++it) {
+      double p0 = 1.0, p1 = x;
+      for (int k = 2; k <= N; ++k) {
+        const double p2 = ((2 * k - 1) * x * p1 - (k - 1) * p0) / k;
+        p0 = p1;
+        p1 = p2;
+      }
+      PN = p1;
+      const double dx = (x * p1 - p0) / ((N + 1) * p1);
+      x -= dx;
+      if (std::fabs(dx) <= 2.2e-16) break;
+    }
+    double p0 = 1.0, p1 = x;  // P_N at the converged node
+    for (int k = 2; k <= N; ++k) {
+      const double p2 = ((2 * k - 1) * x * p1 - (k - 1) * p0) / k;
+      p0 = p1;
+      p1 = p2;
+    }
+    PN = p1;
+    w[N - i] = 2.0 / (N * (N + 1) * PN * PN);
+  }
+}
+
+struct WTab {
+  double w[16];
+};
+// relative tolerance of the affine test: a few hundred ulps of the metric
+// terms that D x gives for an affine map (their round-off grows with N and
+// with the coordinates' magnitude over the element size)
+constexpr double AFFINE_TOL = 1e-10;
+
+// Affine-element records of a mesh (the element layout of the pipelined
+// stage's AFF geometry): per element its metric terms and J at node 0 and per
+// face the unit normal and sJ at face node 0, rounded to T, padded to `gs`
+// values.  An element whose metric, J = MJ / M, normals or sJ = sMJ / sM
+// differ at any node from node 0's by more than `tol` (relative to the
+// element's largest metric term, to J, to 1 for the normals, to sJ) sets
+// *flag: the mesh is then not affine and the records are not used.
+template <typename T>
+__global__ void k_affine(int dim, int Nq, int64_t nelem, const double *vgeo, const double *sgeo, WTab wt, T *out,
+                         int gs, double tol, unsigned *flag) {
+  const int Np = dim == 2 ? Nq * Nq : Nq * Nq * Nq, Nfp = dim == 2 ? Nq : Nq * Nq, nf = 2 * dim;
+  const int nvg = dim == 2 ? 8 : 14, nsg = dim == 2 ? 4 : 5, nm = dim * dim;
+  const double *w = wt.w;
+  const double M0 = dim == 2 ? w[0] * w[0] : (w[0] * w[0]) * w[0];
+  const double sM0 = dim == 2 ? w[0] : w[0] * w[0];
+  for (int64_t e = blockIdx.x; e < nelem; e += gridDim.x) {
+    const double *vg = vgeo + (int64_t)Np * nvg * e;
+    const double *sg = sgeo + (int64_t)nsg * Nfp * nf * e;
+    double scale = 0.0;
+    for (int f = 0; f < nm; ++f) scale = fmax(scale, fabs(vg[(int64_t)Np * f]));
+    const double J0 = vg[(int64_t)Np * nm] / M0;
+    bool bad = !(scale > 0.0) || !(J0 > 0.0);
+    for (int q = threadIdx.x; q < Np; q += blockDim.x) {
+      const int i = q % Nq, j = (q / Nq) % Nq, k = dim == 3 ? q / (Nq * Nq) : 0;
+      const double M = dim == 2 ? w[j] * w[i] : (w[k] * w[j]) * w[i];
+      for (int f = 0; f < nm; ++f)
+        bad |= !(fabs(vg[q + (int64_t)Np * f] - vg[(int64_t)Np * f]) <= tol * scale);
+      bad |= !(fabs(vg[q + (int64_t)Np * nm] - M * J0) <= tol * M * J0);
+    }
+    for (int t = threadIdx.x; t < nf * Nfp; t += blockDim.x) {
+      const int f = t / Nfp, fn = t % Nfp;
+      const double *s = sg + (int64_t)nsg * t, *s0 = sg + (int64_t)nsg * Nfp * f;
+      const double sM = dim == 2 ? w[fn] : w[fn / Nq] * w[fn % Nq];
+      const double sJ0 = s0[dim] / sM0;
+      for (int c = 0; c < dim; ++c) bad |= !(fabs(s[c] - s0[c]) <= tol);
+      bad |= !(fabs(s[dim] - sM * sJ0) <= tol * sM * sJ0);
+    }
+    if (bad) atomicOr(flag, 1u);
+    T *rec = out + (int64_t)gs * e;
+    for (int t = threadIdx.x; t < gs; t += blockDim.x) {
+      double v = 0.0;
+      if (t < nm) v = vg[(int64_t)Np * t];
+      else if (t == nm) v = J0;
+      else if (t < nm + 1 + nf * (dim + 1)) {
+        const int f = (t - nm - 1) / (dim + 1), c = (t - nm - 1) % (dim + 1);
+        const double *s0 = sg + (int64_t)nsg * Nfp * f;
+        v = c < dim ? s0[c] : s0[dim] / sM0;
+      }
+      rec[t] = T(v);
+    }
+  }
+}
+
 __global__ void k_batch_hdr(BHdr *hdr, int sid, BWork *ptr, int nwork) {
   if (threadIdx.x == 0) {
     if (ptr) hdr->work[sid] = ptr;
@@ -94,7 +186,7 @@ BKernels<T> &b_kernels() {
 }
 template <typename T>
 bool b_var_ok(int dim, int N, int var) {
-  return b_order_ok(dim, N) && var >= 0 && var < NVAR && b_kernels<T>().fn[shape_id(dim, N, var)] != nullptr;
+  return b_order_ok(dim, N) && var >= 0 && var < NVAR_SEL && b_kernels<T>().fn[shape_id(dim, N, var)] != nullptr;
 }
 // default variant: the pipelined stage where it is built, else 512-node groups
 // (the autotuner may choose another)
@@ -130,6 +222,9 @@ struct cb_mesh {
   const void *vgeo = nullptr, *sgeo = nullptr, *D = nullptr;
   void *owned = nullptr;  // FP32 copies of vgeo | sgeo | D (precision 32)
   int32_t *nbr = nullptr;
+  // affine-element geometry: [LGL weights | one record per element], in the
+  // mesh's precision; null when some element is not affine
+  void *aff = nullptr;
 };
 
 namespace {
@@ -172,6 +267,7 @@ struct cb_batch {
   std::vector<BSlot> slots;
   int64_t steps = 0;  // batch steps launched (the device counter after them)
   int var[2][BMAXN2 + 1] = {};
+  bool affine = true;  // use the affine-element stage where it applies
   // one step as a graph; re-built when the set of shapes present changes
   cudaGraphExec_t exec = nullptr;
   std::bitset<NSHAPE> g_shapes;
@@ -259,7 +355,8 @@ cudaError_t build_graph(cb_batch *b, const std::bitset<NSHAPE> &shapes) {
   // the pipelined kernels of every (dim, N) take a BatchSrc whose layout does
   // not depend on its template arguments
   using SrcArgs = BatchSrc<T, 5, 1>;
-  static_assert(sizeof(SrcArgs) == sizeof(BatchSrc<T, 4, 64>), "BatchSrc layout");
+  static_assert(sizeof(SrcArgs) == sizeof(BatchSrc<T, 4, 64>) && sizeof(SrcArgs) == sizeof(BatchSrc<T, 4, 64, 4>),
+                "BatchSrc layout");
   for (int sid = 0; sid < NSHAPE && e == cudaSuccess; ++sid) {
     if (!shapes.test(sid)) continue;
     if ((e = b_prepare<T>(sid)) != cudaSuccess) break;
@@ -341,8 +438,12 @@ int batch_add(cb_batch *b, const cb_mesh *m, void *Q, void *rhs, double dt, int6
   const int Nq = m->N + 1, ns = m->dim == 2 ? 4 : 5;
   const int64_t Np = m->dim == 2 ? (int64_t)Nq * Nq : (int64_t)Nq * Nq * Nq;
   const int var = b->var[m->dim - 2][m->N];
-  const int sid = shape_id(m->dim, m->N, var);
-  const int epb = b_kernels<T>().epb[sid];
+  int sid = shape_id(m->dim, m->N, var);
+  const BKernels<T> &K = b_kernels<T>();
+  const bool aff = b->affine && m->aff && b->phys.gravity == 0.0 && K.pipelined[sid] &&
+                   K.fn[shape_id(m->dim, m->N, VAR_AFFINE)];
+  if (aff) sid = shape_id(m->dim, m->N, VAR_AFFINE);
+  const int epb = K.epb[sid];
   const int64_t ngroups = (m->nelem + epb - 1) / epb;
   const size_t qbytes = sizeof(T) * Np * ns * m->nelem;
   void *alt = nullptr;
@@ -356,7 +457,7 @@ int batch_add(cb_batch *b, const cb_mesh *m, void *Q, void *rhs, double dt, int6
   sl.used = true;
   sl.dim = m->dim;
   sl.N = m->N;
-  sl.var = var;
+  sl.var = aff ? VAR_AFFINE : var;
   sl.sid = sid;
   sl.epb = epb;
   sl.nelem = m->nelem;
@@ -370,7 +471,7 @@ int batch_add(cb_batch *b, const cb_mesh *m, void *Q, void *rhs, double dt, int6
   d.Q[0] = (T *)Q;
   d.Q[1] = (T *)alt;
   d.rhs = (T *)rhs;
-  d.vgeo = (const T *)m->vgeo;
+  d.vgeo = (const T *)(aff ? m->aff : m->vgeo);
   d.sgeo = (const T *)m->sgeo;
   d.D = (const T *)m->D;
   d.nbr = m->nbr;
@@ -439,13 +540,13 @@ int cb_mesh_create(cb_mesh **out, int dim, int N, int precision, int64_t nelem, 
   const int64_t Np = dim == 2 ? (int64_t)Nq * Nq : (int64_t)Nq * Nq * Nq, Nfp = dim == 2 ? Nq : (int64_t)Nq * Nq;
   unsigned *status = nullptr;
   cudaError_t e = cudaMalloc((void **)&m->nbr, sizeof(int32_t) * 2 * dim * nelem);
-  if (e == cudaSuccess) e = cudaMalloc((void **)&status, sizeof(unsigned));
+  if (e == cudaSuccess) e = cudaMalloc((void **)&status, 2 * sizeof(unsigned));
   if (e != cudaSuccess) {
     cb_mesh_destroy(m);
     cudaFree(status);
     return solver_fail(CB_ERR_NOMEM, "cb_mesh_create: %s", cudaGetErrorString(e));
   }
-  cudaMemsetAsync(status, 0, sizeof(unsigned), st);
+  cudaMemsetAsync(status, 0, 2 * sizeof(unsigned), st);
   const Ops<double> *o = dim == 2 ? get_ops<2, double>(N) : get_ops<3, double>(N);
   e = o->build_nbr(m->nbr, vmapM, vmapP, elemtobndy, nelem, status, st);
   if (e == cudaSuccess && precision == 32) {
@@ -465,10 +566,42 @@ int cb_mesh_create(cb_mesh **out, int dim, int N, int precision, int64_t nelem, 
     m->sgeo = sgeo;
     m->D = D;
   }
-  unsigned h = 0;
-  if (e == cudaSuccess && (e = cudaMemcpyAsync(&h, status, sizeof h, cudaMemcpyDeviceToHost, st)) == cudaSuccess)
+  // affine-element records (status bit 31 set: some element is not affine)
+  const size_t wsz = precision == 64 ? 8 : 4;
+  const int aw = dim * dim + 1 + 2 * dim * (dim + 1);
+  const int64_t gs = (int64_t)((wsz * aw + 15) & ~size_t(15)) / wsz, woff = (int64_t)((wsz * Nq + 15) & ~size_t(15)) / wsz;
+  double wl[16] = {};
+  lgl_weights(N, wl);
+  if (e == cudaSuccess) e = cudaMalloc(&m->aff, wsz * (woff + gs * nelem));
+  if (e == cudaSuccess) {
+    WTab wt{};
+    float wf[16] = {};
+    for (int i = 0; i < Nq; ++i) {
+      wt.w[i] = wl[i];
+      wf[i] = (float)wl[i];
+    }
+    e = cudaMemcpyAsync(m->aff, precision == 64 ? (const void *)wt.w : (const void *)wf, wsz * Nq,
+                        cudaMemcpyHostToDevice, st);
+    const int blocks = (int)std::min<int64_t>(nelem, 4096);
+    if (e == cudaSuccess) {
+      if (precision == 64)
+        k_affine<double><<<blocks, 128, 0, st>>>(dim, Nq, nelem, vgeo, sgeo, wt, (double *)m->aff + woff, (int)gs,
+                                                 AFFINE_TOL, status + 1);
+      else
+        k_affine<float><<<blocks, 128, 0, st>>>(dim, Nq, nelem, vgeo, sgeo, wt, (float *)m->aff + woff, (int)gs,
+                                                AFFINE_TOL, status + 1);
+      e = cudaGetLastError();
+    }
+  }
+  unsigned h = 0, ha = 0;
+  if (e == cudaSuccess && (e = cudaMemcpyAsync(&h, status, sizeof h, cudaMemcpyDeviceToHost, st)) == cudaSuccess &&
+      (e = cudaMemcpyAsync(&ha, status + 1, sizeof ha, cudaMemcpyDeviceToHost, st)) == cudaSuccess)
     e = cudaStreamSynchronize(st);
   cudaFree(status);
+  if (e == cudaSuccess && ha) {
+    cudaFree(m->aff);
+    m->aff = nullptr;
+  }
   if (e != cudaSuccess) {
     cb_mesh_destroy(m);
     return solver_fail(CB_ERR_CUDA, "cb_mesh_create: %s", cudaGetErrorString(e));
@@ -482,10 +615,17 @@ int cb_mesh_create(cb_mesh **out, int dim, int N, int precision, int64_t nelem, 
   return CB_OK;
 }
 
+int cb_mesh_affine(const cb_mesh *m, int *affine) {
+  if (!m || !affine) return solver_fail(CB_ERR_ARG, "cb_mesh_affine: null argument");
+  *affine = m->aff != nullptr;
+  return CB_OK;
+}
+
 int cb_mesh_destroy(cb_mesh *m) {
   if (!m) return CB_OK;
   cudaFree(m->nbr);
   cudaFree(m->owned);
+  cudaFree(m->aff);
   delete m;
   return CB_OK;
 }
@@ -554,6 +694,12 @@ int cb_batch_set_variant(cb_batch *b, int dim, int N, int variant) {
   return CB_OK;
 }
 
+int cb_batch_set_affine(cb_batch *b, int on) {
+  if (!b) return solver_fail(CB_ERR_ARG, "cb_batch_set_affine: null handle");
+  b->affine = on != 0;
+  return CB_OK;
+}
+
 int cb_batch_get_variant(const cb_batch *b, int dim, int N, int *variant) {
   if (!b || !variant || (dim != 2 && dim != 3) || !b_order_ok(dim, N))
     return solver_fail(CB_ERR_ARG, "cb_batch_get_variant: bad arguments");
@@ -581,6 +727,13 @@ int cb_batch_info(const cb_batch *b, int slot, int64_t *done, int64_t *target) {
   const BSlot &s = b->slots[slot];
   if (done) *done = std::min(s.target, b->steps - s.start);
   if (target) *target = s.target;
+  return CB_OK;
+}
+
+int cb_batch_slot_variant(const cb_batch *b, int slot, int *variant) {
+  if (!b || !variant || slot < 0 || slot >= b->cap || !b->slots[slot].used)
+    return solver_fail(CB_ERR_ARG, "cb_batch_slot_variant: slot is not in use");
+  *variant = b->slots[slot].var;
   return CB_OK;
 }
 

@@ -57,7 +57,12 @@ struct alignas(16) BWork {
 // occupancies among 2, 3 and 4 blocks per SM (blocks of up to 256 threads).
 // Shape id of (dim, N, variant); ids of shapes that are not built stay
 // unused.
-constexpr int NVAR = 5;
+// Stage variants per (dim, N): 0 pipelined (default occupancy), 1 / 2
+// grouped (~256 / ~512 nodes), 3 / 4 pipelined at other occupancies — the
+// ones a caller may select — and VAR_AFFINE, the pipelined stage with
+// affine-element geometry, which the batch uses in place of a pipelined
+// variant for meshes whose elements are all affine (gravity off).
+constexpr int NVAR_SEL = 5, VAR_AFFINE = 5, NVAR = 6;
 constexpr int NSHAPE = 2 * NVAR * (BMAXN2 + 1);
 __host__ __device__ constexpr int shape_id(int dim, int N, int var) {
   return (dim - 2) * NVAR * (BMAXN2 + 1) + NVAR * N + var;
@@ -220,7 +225,8 @@ k_stage_batch(const BHdr *__restrict__ hdr, int stage, PhysT<T> p, T rka, double
 // Item source of the pipelined stage over a work list of many instances
 // (see k_stage_pipe2).  The second warp of the block (the first issues the
 // bulk copies) finds the block's next live item and publishes it into a
-// three-entry shared-memory ring (current, next, and the one being published):
+// shared-memory ring (the current item, the ones whose copies are in flight,
+// and the one being published; three entries, four for the DEEP stage):
 // each lane copies one 8-byte word of the instance descriptor, so a publish
 // costs two parallel round trips (work item, descriptor).  The shape's list,
 // the descriptor table and the batch step are cached at the head of the ring.
@@ -236,13 +242,17 @@ struct alignas(16) BRingHdr {
   int64_t step;
   int32_t nwork, pad;
 };
-template <typename T, int NS, int EPB>
+// RING: ring entries; items it .. it + RING - 2 are published at the top of
+// iteration it (the group in work and RING - 2 ahead of it), and publish(it)
+// writes item it + RING - 1.
+template <typename T, int NS, int EPB, int RING = 3>
 struct BatchSrc {
   static constexpr int WORDS = (int)(sizeof(BDesc<T>) / 8);
   static_assert(sizeof(BDesc<T>) % 8 == 0 && WORDS <= 32, "descriptor words");
   static constexpr int START_WORD = (int)(offsetof(BDesc<T>, start) / 8);
   static constexpr int TARGET_WORD = (int)(offsetof(BDesc<T>, target) / 8);
-  static constexpr size_t RING_BYTES = sizeof(BRingHdr) + 3 * sizeof(BItem<T>);
+  static constexpr int AHEAD = RING - 2;
+  static constexpr size_t RING_BYTES = sizeof(BRingHdr) + RING * sizeof(BItem<T>);
   static constexpr int PUBLISHER = 32;  // first thread of the publishing warp
   const BHdr *hdr;
   int sid, stage;
@@ -289,9 +299,12 @@ struct BatchSrc {
         rh->nwork = hdr->nwork[sid];
       }
       __syncwarp();
-      const int w0 = publish_from(blockIdx.x, ring[0]);
-      const int w1 = w0 < 0 ? -1 : publish_from(w0 + gridDim.x, ring[1]);
-      wpos = w1;
+      int w = publish_from(blockIdx.x, ring[0]);
+      for (int j = 1; j < RING - 1; ++j) {
+        if (w >= 0) w = publish_from(w + gridDim.x, ring[j]);
+        else if ((threadIdx.x & 31) == 0) ring[j].valid = 0;
+      }
+      wpos = w;
     }
   }
   // start fetching the work item that publish() will most likely read (the
@@ -303,10 +316,10 @@ struct BatchSrc {
     asm volatile("prefetch.global.L1 [%0];" ::"l"(rh->work + w));
   }
   __device__ void publish(int it) {
-    wpos = wpos < 0 ? -1 : publish_from(wpos + gridDim.x, ring[(it + 2) % 3]);
-    if (wpos < 0 && (threadIdx.x & 31) == 0) ring[(it + 2) % 3].valid = 0;
+    wpos = wpos < 0 ? -1 : publish_from(wpos + gridDim.x, ring[(it + RING - 1) % RING]);
+    if (wpos < 0 && (threadIdx.x & 31) == 0) ring[(it + RING - 1) % RING].valid = 0;
   }
-  __device__ const BItem<T> &at(int it) const { return ring[it % 3]; }
+  __device__ const BItem<T> &at(int it) const { return ring[it % RING]; }
   __device__ bool valid(int it) const { return at(it).valid != 0; }
   __device__ int64_t e0(int it) const { return at(it).e0; }
   __device__ int nv(int it) const { return at(it).nv; }
@@ -321,8 +334,8 @@ struct BatchSrc {
   __device__ T rkbdt(int it) const { return T(rkb * at(it).d.dt); }
   __device__ unsigned *status(int it) const { return at(it).d.status; }
 };
-template <int DIM, int Nq, typename T>
-using BPipeSrc = BatchSrc<T, Lay<DIM>::NS, Cfg<DIM, Nq>::EPB>;
+template <int DIM, int Nq, typename T, int RING = 3>
+using BPipeSrc = BatchSrc<T, Lay<DIM>::NS, Cfg<DIM, Nq>::EPB, RING>;
 
 inline bool b_order_ok(int dim, int N) { return N >= 1 && N <= (dim == 2 ? BMAXN2 : BMAXN3); }
 
@@ -342,13 +355,14 @@ constexpr size_t b_group_smem() {
   return sizeof(T) * (((Nq * Nq + 1) & ~1) + (size_t)Lay<DIM>::NS * C::SLOTS +
                       (size_t)DIM * Lay<DIM>::NS * C::SLOTS);
 }
-template <int DIM, int Nq, typename T, int MINB>
+template <int DIM, int Nq, typename T, int MINB, bool AFF = false, bool DEEP = false>
 void b_fill_pipe(BKernels<T> &k, int var) {
+  using Src = BPipeSrc<DIM, Nq, T, DEEP ? 4 : 3>;
   const int id = shape_id(DIM, Nq - 1, var);
-  k.fn[id] = (const void *)k_stage_pipe2<DIM, Nq, T, BPipeSrc<DIM, Nq, T>, MINB>;
+  k.fn[id] = (const void *)k_stage_pipe2<DIM, Nq, T, Src, MINB, AFF, DEEP>;
   k.epb[id] = Cfg<DIM, Nq>::EPB;
   k.threads[id] = Cfg<DIM, Nq>::THREADS;
-  k.smem[id] = Pipe2<DIM, Nq, T>::smem() + BPipeSrc<DIM, Nq, T>::RING_BYTES;
+  k.smem[id] = Pipe2<DIM, Nq, T, AFF, DEEP>::smem() + Src::RING_BYTES;
   k.pipelined[id] = true;
 }
 template <int DIM, int Nq, typename T>
@@ -362,6 +376,10 @@ void b_fill(BKernels<T> &k) {
       b_fill_pipe<DIM, Nq, T, M0 == 3 ? 2 : 3>(k, 3);
       b_fill_pipe<DIM, Nq, T, M0 == 4 ? 2 : 4>(k, 4);
     }
+    // the affine stage copies two groups ahead where that fits M0 blocks per SM
+    using PD = Pipe2<DIM, Nq, T, true, true>;
+    if constexpr (PD::OK && PD::fits(M0)) b_fill_pipe<DIM, Nq, T, M0, true, true>(k, VAR_AFFINE);
+    else if constexpr (Pipe2<DIM, Nq, T, true>::OK) b_fill_pipe<DIM, Nq, T, M0, true>(k, VAR_AFFINE);
   }
   {
     const int id = shape_id(DIM, N, 1);

@@ -6,7 +6,8 @@
 //     refilled with the next group by a bulk copy issued right after the
 //     mid-iteration barrier and lands while phase B runs;
 //   * slabs T[0], T[1] (residual carry + face geometry sgeo) are double
-//     buffered and fetched one group ahead;
+//     buffered and fetched one group ahead (DEEP: two S and three T slabs,
+//     copies two groups ahead);
 //   * neighbour traces are prefetched into registers, their neighbour codes
 //     one group ahead.
 // Used when every slab is a multiple of 16 bytes (bulk copies) and the
@@ -27,7 +28,20 @@
 
 namespace cb {
 
-template <int DIM, int Nq, typename T>
+// AFF: affine-element geometry.  Instead of the per-node metric (vgeo) and
+// per-face-node face geometry (sgeo), every element has one record of AW
+// values — its metric terms, J, and per face the unit normal and sJ — and
+// MJ, MJI and sMJ are formed from the LGL weights as computegeometry does
+// (euler3d_set3c.jl:222-246).  The geometry array is then
+// [w (Nq, padded to 16 bytes) | record of element 0 | record of element 1 ...]
+// (built by cb_mesh_create for meshes whose elements are all affine).
+//
+// DEEP: copies run two groups ahead instead of one — two S slabs (S of group
+// it + 2 is issued when group it releases its slab) and three T slabs (T of
+// group it + 2 is issued at the top of iteration it) — so that a block keeps
+// about twice the bytes in flight, for small groups whose copy latency a
+// single group of work does not cover.
+template <int DIM, int Nq, typename T, bool AFF = false, bool DEEP = false>
 struct Pipe2 {
   using C = Cfg<DIM, Nq>;
   using P1 = Pipe<DIM, Nq, T>;
@@ -35,19 +49,25 @@ struct Pipe2 {
   static constexpr int NG = P1::NG, RS = P1::RS, NR = P1::NR, MV = P1::MV;
   static constexpr size_t QB = P1::QB, GB = P1::GB;
   static constexpr size_t pad16(size_t b) { return (b + 15) & ~size_t(15); }
+  static constexpr int AW = DIM * DIM + 1 + 2 * DIM * (DIM + 1);  // affine record values
+  static constexpr size_t AGB = pad16(sizeof(T) * AW);             // affine record bytes
+  static constexpr int WOFF = (int)(pad16(sizeof(T) * Nq) / sizeof(T));  // records after the weights
   // the metric fields of an element are copied as one padded run (the pad
   // reads the start of the coordinate fields, which are never used)
-  static constexpr size_t GBP = pad16(GB);
-  static constexpr int GS = (int)(GBP / sizeof(T));  // element stride of the staged metric
+  static constexpr size_t GBP = AFF ? AGB : pad16(GB);
+  static constexpr int GS = (int)(GBP / sizeof(T));  // element stride of the staged metric / record
   static constexpr size_t VB = sizeof(T) * (size_t)C::Np * NVG;  // vgeo bytes per element
-  static constexpr size_t SB = sizeof(T) * (size_t)NSG * C::Nfp * C::NFACE;  // sgeo per element
-  static constexpr bool BULK = QB % 16 == 0 && VB % 16 == 0 && SB % 16 == 0 && GBP <= VB;
-  static constexpr size_t OFF_D = 32;  // 3 mbarriers before
+  static constexpr size_t SB = AFF ? 0 : sizeof(T) * (size_t)NSG * C::Nfp * C::NFACE;  // sgeo per element
+  static constexpr bool BULK =
+      AFF ? QB % 16 == 0 : (QB % 16 == 0 && VB % 16 == 0 && SB % 16 == 0 && GBP <= VB);
+  static constexpr int NSB = DEEP ? 2 : 1, NTB = DEEP ? 3 : 2;  // S and T slabs
+  static constexpr int LOOK = DEEP ? 2 : 1;  // groups ahead whose copies are issued
+  static constexpr size_t OFF_D = DEEP ? 48 : 32;  // NSB + NTB mbarriers before
   static constexpr size_t OFF_S = OFF_D + pad16(sizeof(T) * Nq * RS);
   static constexpr size_t SBYTES = C::EPB * (QB + GBP);
-  static constexpr size_t OFF_T = OFF_S + pad16(SBYTES);
+  static constexpr size_t OFF_T = OFF_S + NSB * pad16(SBYTES);
   static constexpr size_t TBYTES = C::EPB * (QB + SB);
-  static constexpr size_t OFF_F = OFF_T + 2 * pad16(TBYTES);
+  static constexpr size_t OFF_F = OFF_T + NTB * pad16(TBYTES);
   static constexpr size_t FDIR = P1::FDIR;
   static constexpr size_t FLUX = sizeof(T) * DIM * FDIR;
   static constexpr size_t OFF_FF = OFF_F + pad16(FLUX);
@@ -57,6 +77,9 @@ struct Pipe2 {
   static constexpr bool OK = BULK && smem() + RING_MAX <= SMEM_LIMIT;
   // blocks of up to 256 threads are sized for two (FP64) or four (FP32) per SM
   static constexpr int MINB = C::THREADS <= 256 ? (sizeof(T) == 4 ? 4 : 2) : 1;
+  // whether `blocks` blocks fit in one SM's shared memory (228 KB, 1 KB of
+  // it reserved per block)
+  static constexpr bool fits(int blocks) { return blocks * (smem() + RING_MAX + 1024) <= 228 * 1024; }
 };
 
 // One mesh: groups of EPB consecutive elements, pointers and constants are
@@ -65,6 +88,7 @@ template <typename T, int NS, int EPB>
 struct MeshSrc {
   static constexpr size_t RING_BYTES = 0;
   static constexpr int PUBLISHER = 0;
+  static constexpr int AHEAD = 1 << 20;  // groups ahead known at the top of an iteration
   const T *Qin_;
   T *Qout_, *rhs_;
   const T *vgeo_, *sgeo_;
@@ -96,37 +120,46 @@ struct MeshSrc {
   __device__ unsigned *status(int) const { return status_; }
 };
 
-// MINB: resident blocks per SM that the register allocation is sized for.
-template <int DIM, int Nq, typename T, typename Src, int MINB = Pipe2<DIM, Nq, T>::MINB>
+// MINB: resident blocks per SM that the register allocation is sized for;
+// AFF: affine-element geometry (see Pipe2; gravity must be zero); DEEP:
+// copies two groups ahead (see Pipe2).
+template <int DIM, int Nq, typename T, typename Src, int MINB = Pipe2<DIM, Nq, T>::MINB, bool AFF = false,
+          bool DEEP = false>
 __global__ void __launch_bounds__(Cfg<DIM, Nq>::THREADS, MINB)
 k_stage_pipe2(Src src, PhysT<T> p, T rka) {
   using C = Cfg<DIM, Nq>;
-  using PP = Pipe2<DIM, Nq, T>;
+  using PP = Pipe2<DIM, Nq, T, AFF, DEEP>;
+  static_assert(Src::AHEAD >= PP::LOOK, "the source must publish the groups whose copies are issued");
   constexpr int NS = Lay<DIM>::NS, NVG = Lay<DIM>::NVG, NSG = Lay<DIM>::NSG, IR = Lay<DIM>::IR;
   constexpr int Np = C::Np, Nfp = C::Nfp, NF = C::NFACE, EPB = C::EPB, SP = C::SLOTS;
   constexpr int MJI = DIM * DIM + 1, GC = DIM * DIM + 2 + DIM - 1;
   constexpr int FS = EPB * Nfp, RS = PP::RS, NR = PP::NR, GS = PP::GS;
   constexpr size_t TSTRIDE = PP::pad16(PP::TBYTES) / sizeof(T);
+  constexpr size_t SSTRIDE = PP::pad16(PP::SBYTES) / sizeof(T);
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  uint64_t *barS = reinterpret_cast<uint64_t *>(smem_raw);
-  uint64_t *barT = barS + 1;  // barT[0], barT[1]
+  uint64_t *barS = reinterpret_cast<uint64_t *>(smem_raw);  // barS[NSB]
+  uint64_t *barT = barS + PP::NSB;                         // barT[NTB]
   T *DT = reinterpret_cast<T *>(smem_raw + PP::OFF_D);
-  T *Sq = reinterpret_cast<T *>(smem_raw + PP::OFF_S);  // [EPB][NS][Np]
-  T *Sg = Sq + EPB * Np * NS;                             // [EPB][GS]: metric, MJ, MJI rows
-  T *T0 = reinterpret_cast<T *>(smem_raw + PP::OFF_T);   // [EPB][NS][Np] carry, then [EPB] sgeo
+  T *S0 = reinterpret_cast<T *>(smem_raw + PP::OFF_S);  // per slab [EPB][NS][Np] state, then [EPB][GS]
+  T *T0 = reinterpret_cast<T *>(smem_raw + PP::OFF_T);  // per slab [EPB][NS][Np] carry, then [EPB] sgeo
   T *sF = reinterpret_cast<T *>(smem_raw + PP::OFF_F);
   T *FF = reinterpret_cast<T *>(smem_raw + PP::OFF_FF);
   const int tid = threadIdx.x;
 
-  auto issue_S = [&](int it) {  // thread 0 only
+  auto issue_S = [&](int it, int b) {  // thread 0 only
     const int64_t e0 = src.e0(it);
     const int nv = src.nv(it);
     const T *q = src.Qin(it), *vg = src.vgeo(it);
+    T *dq = S0 + b * SSTRIDE, *dg = dq + EPB * Np * NS;
     fence_proxy_async();
-    mbar_expect_tx(barS, (uint32_t)(nv * (PP::QB + PP::GBP)));
-    bulk_g2s(Sq, q + e0 * Np * NS, (uint32_t)(nv * PP::QB), barS);
-    for (int el = 0; el < nv; ++el)
-      bulk_g2s(Sg + el * GS, vg + (e0 + el) * Np * NVG, (uint32_t)PP::GBP, barS);
+    mbar_expect_tx(&barS[b], (uint32_t)(nv * (PP::QB + PP::GBP)));
+    bulk_g2s(dq, q + e0 * Np * NS, (uint32_t)(nv * PP::QB), &barS[b]);
+    if constexpr (AFF) {  // the group's records are contiguous
+      bulk_g2s(dg, vg + PP::WOFF + e0 * GS, (uint32_t)(nv * PP::GBP), &barS[b]);
+    } else {
+      for (int el = 0; el < nv; ++el)
+        bulk_g2s(dg + el * GS, vg + (e0 + el) * Np * NVG, (uint32_t)PP::GBP, &barS[b]);
+    }
   };
   auto issue_T = [&](int it, int b) {  // thread 0 only
     const int64_t e0 = src.e0(it);
@@ -135,24 +168,24 @@ k_stage_pipe2(Src src, PhysT<T> p, T rka) {
     fence_proxy_async();
     mbar_expect_tx(&barT[b], (uint32_t)(nv * (PP::QB + PP::SB)));
     bulk_g2s(dc, src.rhs(it) + e0 * Np * NS, (uint32_t)(nv * PP::QB), &barT[b]);
-    bulk_g2s(ds, src.sgeo(it) + e0 * (PP::SB / sizeof(T)), (uint32_t)(nv * PP::SB), &barT[b]);
+    if constexpr (!AFF)
+      bulk_g2s(ds, src.sgeo(it) + e0 * (PP::SB / sizeof(T)), (uint32_t)(nv * PP::SB), &barT[b]);
   };
 
   src.begin(smem_raw + PP::smem());
   if (tid == 0) {
-    mbar_init(barS, 1);
-    mbar_init(&barT[0], 1);
-    mbar_init(&barT[1], 1);
+    for (int b = 0; b < PP::NSB + PP::NTB; ++b) mbar_init(&barS[b], 1);
     fence_mbar_init();
   }
   if constexpr (PP::MV > Nq)
     for (size_t t = tid; t < (size_t)DIM * PP::FDIR; t += C::THREADS)
       if ((int)(t % RS) >= Nq) sF[t] = T(0);
   __syncthreads();
-  if (tid == 0 && src.valid(0)) {
-    issue_S(0);
-    issue_T(0, 0);
-  }
+  if (tid == 0)
+    for (int j = 0; j < PP::LOOK && src.valid(j); ++j) {
+      issue_S(j, j);
+      issue_T(j, j);
+    }
 
   int32_t nbn[C::FPT];
   auto load_nbr = [&](int it, int32_t *dst) {
@@ -172,11 +205,11 @@ k_stage_pipe2(Src src, PhysT<T> p, T rka) {
   bool timed_out = false;
   const T *curD = nullptr;  // derivative matrix held in DT (rows padded like the flux rows)
   for (int it = 0; src.valid(it); ++it) {
-    const int b = it & 1;
+    const int sb = it % PP::NSB, tb = it % PP::NTB;
     const int64_t e0 = src.e0(it);
     const int nv = src.nv(it);
-    const bool more = src.valid(it + 1);
-    if (tid == 0 && more) issue_T(it + 1, b ^ 1);
+    const bool more = src.valid(it + PP::LOOK);  // a group whose copies are issued in this iteration
+    if (tid == 0 && more) issue_T(it + PP::LOOK, (it + PP::LOOK) % PP::NTB);
     if (tid == Src::PUBLISHER) src.prefetch();
     const T *__restrict__ Qin = src.Qin(it);
     T qr[NS];
@@ -201,10 +234,11 @@ k_stage_pipe2(Src src, PhysT<T> p, T rka) {
       }
     }
 
-    // ---- wait for S (state + metric) and T[b] (carry + sgeo)
-    if (!mbar_wait_bounded(barS, (uint32_t)(it & 1), WAIT_LIMIT)) timed_out = true;
-    if (!mbar_wait_bounded(&barT[b], (uint32_t)((it >> 1) & 1), WAIT_LIMIT)) timed_out = true;
-    const T *Tc = T0 + b * TSTRIDE, *Ts = Tc + EPB * Np * NS;
+    // ---- wait for S[sb] (state + metric) and T[tb] (carry + sgeo)
+    if (!mbar_wait_bounded(&barS[sb], (uint32_t)((it / PP::NSB) & 1), WAIT_LIMIT)) timed_out = true;
+    if (!mbar_wait_bounded(&barT[tb], (uint32_t)((it / PP::NTB) & 1), WAIT_LIMIT)) timed_out = true;
+    const T *Sq = S0 + sb * SSTRIDE, *Sg = Sq + EPB * Np * NS;
+    const T *Tc = T0 + tb * TSTRIDE, *Ts = Tc + EPB * Np * NS;
     const T *__restrict__ vgeo = src.vgeo(it);
     if (src.D(it) != curD) {  // read in phase B only; visible after the mid barrier
       curD = src.D(it);
@@ -230,19 +264,30 @@ k_stage_pipe2(Src src, PhysT<T> p, T rka) {
           q[s] = qd[u][s] + qr[s];
         }
         const T *G = Sg + el * GS;
-        T met[DIM][DIM];
+        const int i = n % Nq, j = (n / Nq) % Nq, k = DIM == 3 ? n / (Nq * Nq) : 0;
+        T met[DIM][DIM], MJ, gc = T(0);
+        if constexpr (AFF) {
 #pragma unroll
-        for (int r = 0; r < DIM; ++r)
+          for (int r = 0; r < DIM; ++r)
 #pragma unroll
-          for (int c = 0; c < DIM; ++c) met[r][c] = G[(r + DIM * c) * Np + n];
-        const T MJ = G[DIM * DIM * Np + n];
-        mji[u] = G[MJI * Np + n];
-        const T gc = p.grav != T(0) ? vgeo[n + Np * (GC + NVG * (e0 + el))] : T(0);
+            for (int c = 0; c < DIM; ++c) met[r][c] = G[r + DIM * c];
+          // M = kron(w, w[, w]) in computegeometry's multiplication order
+          const T M = DIM == 2 ? vgeo[j] * vgeo[i] : (vgeo[k] * vgeo[j]) * vgeo[i];
+          MJ = M * G[DIM * DIM];
+          mji[u] = T(1) / MJ;
+        } else {
+#pragma unroll
+          for (int r = 0; r < DIM; ++r)
+#pragma unroll
+            for (int c = 0; c < DIM; ++c) met[r][c] = G[(r + DIM * c) * Np + n];
+          MJ = G[DIM * DIM * Np + n];
+          mji[u] = G[MJI * Np + n];
+          gc = p.grav != T(0) ? vgeo[n + Np * (GC + NVG * (e0 + el))] : T(0);
+        }
         const T ri = T(1) / q[IR];
         const T P = pressure_ri<DIM, T>(q, ri, gc, p);
         T f[NS][DIM];
         euler_flux_ri<DIM, T>(q, ri, P, f);
-        const int i = n % Nq, j = (n / Nq) % Nq, k = DIM == 3 ? n / (Nq * Nq) : 0;
 #pragma unroll
         for (int r = 0; r < DIM; ++r) {
           const int row = DIM == 2 ? (r == 0 ? j : i) : (r == 0 ? j + Nq * k : (r == 1 ? i + Nq * k : i + Nq * j));
@@ -262,16 +307,24 @@ k_stage_pipe2(Src src, PhysT<T> p, T rka) {
       const int fs = tid + u * C::THREADS;
       const int el = fs / (NF * Nfp), f = (fs / Nfp) % NF, fn = fs % Nfp;
       if (fs < C::FSLOTS && el < nv) {
-        const T *sg = Ts + (size_t)NSG * (fn + Nfp * (f + NF * el));
-        T nrm[DIM];
+        T nrm[DIM], smj;
+        if constexpr (AFF) {
+          const T *rec = Sg + el * GS + DIM * DIM + 1 + f * (DIM + 1);
 #pragma unroll
-        for (int c = 0; c < DIM; ++c) nrm[c] = sg[c];
-        const T smj = sg[DIM];
+          for (int c = 0; c < DIM; ++c) nrm[c] = rec[c];
+          const T sM = DIM == 2 ? vgeo[fn] : vgeo[fn / Nq] * vgeo[fn % Nq];
+          smj = sM * rec[DIM];
+        } else {
+          const T *sg = Ts + (size_t)NSG * (fn + Nfp * (f + NF * el));
+#pragma unroll
+          for (int c = 0; c < DIM; ++c) nrm[c] = sg[c];
+          smj = sg[DIM];
+        }
         const int vM = face_node<DIM, Nq>(f, fn);
         T qM[NS], qq[NS];
 #pragma unroll
         for (int s = 0; s < NS; ++s) qM[s] = Sq[(el * NS + s) * Np + vM] + qr[s];
-        const T gM = p.grav != T(0) ? vgeo[vM + Np * (GC + NVG * (e0 + el))] : T(0);
+        const T gM = (!AFF && p.grav != T(0)) ? vgeo[vM + Np * (GC + NVG * (e0 + el))] : T(0);
         const T riM = T(1) / qM[IR];
         const T PM = pressure_ri<DIM, T>(qM, riM, gM, p);
         T PPv, riP;
@@ -279,7 +332,7 @@ k_stage_pipe2(Src src, PhysT<T> p, T rka) {
 #pragma unroll
           for (int s = 0; s < NS; ++s) qq[s] = qP[u][s];
           T gP = T(0);
-          if (p.grav != T(0)) {
+          if (!AFF && p.grav != T(0)) {
             const int64_t e2 = nbv[u] >> 3;
             gP = vgeo[face_node<DIM, Nq>(nbv[u] & 7, fn) + Np * (GC + NVG * e2)];
           }
@@ -297,8 +350,8 @@ k_stage_pipe2(Src src, PhysT<T> p, T rka) {
       }
     }
     __syncthreads();
-    // S is no longer read: refill it with the next group while phase B runs
-    if (tid == 0 && more) issue_S(it + 1);
+    // S[sb] is no longer read: refill it while phase B runs
+    if (tid == 0 && more) issue_S(it + PP::LOOK, sb);
     if ((tid >> 5) == (Src::PUBLISHER >> 5)) src.publish(it);
     // ---- phase B: carry - source + volume contraction - face terms, update
     T *__restrict__ Qout = src.Qout(it);
@@ -331,7 +384,7 @@ k_stage_pipe2(Src src, PhysT<T> p, T rka) {
       atomicOr(src.status(it), ST_TIMEOUT);
       timed_out = false;
     }
-    __syncthreads();  // T[b], the flux rows, FF and the item ring are free for reuse
+    __syncthreads();  // T[tb], the flux rows, FF and the item ring are free for reuse
   }
 }
 

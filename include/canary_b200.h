@@ -228,6 +228,13 @@ int cb_mesh_create(cb_mesh **out, int dim, int N, int precision,
                    const int64_t *vmapM, const int64_t *vmapP,
                    const int64_t *elemtobndy, const double *D,
                    cb_stream_t stream);
+/* Whether every element of the mesh is affine: its metric terms, J (MJ / M),
+ * unit normals and sJ (sMJ / sM) equal their values at the first node to a
+ * relative 1e-10.  cb_mesh_create then also keeps one record per element
+ * (metric, J, per face normal and sJ), and the pipelined batch stage forms
+ * MJ, MJI and sMJ from the LGL weights as computegeometry does
+ * (euler3d_set3c.jl:222-246) instead of reading the per-node geometry. */
+int cb_mesh_affine(const cb_mesh *m, int *affine);
 int cb_mesh_destroy(cb_mesh *m);
 
 /* A batch of up to max_instances slots.  All calls are ordered on `stream`
@@ -246,6 +253,11 @@ int cb_batch_create(cb_batch **out, int precision, int max_instances,
  * the grouped ones, and the two families to round-off. */
 int cb_batch_set_variant(cb_batch *b, int dim, int N, int variant);
 int cb_batch_get_variant(const cb_batch *b, int dim, int N, int *variant);
+/* Instances admitted from now on whose mesh is affine (cb_mesh_affine), with
+ * gravity 0 and a pipelined variant selected, use the affine-element stage
+ * when `on` (the default); it agrees with the per-node geometry to
+ * round-off and reads no vgeo / sgeo. */
+int cb_batch_set_affine(cb_batch *b, int on);
 /* Admit an instance: the caller's state Q and zeroed residual carry rhs
  * (layouts as above, precision of the batch) advance by nsteps steps of dt
  * during the following cb_batch_run calls.  qref (nstate doubles, or NULL for
@@ -260,6 +272,9 @@ int cb_batch_add(cb_batch *b, const cb_mesh *m, void *Q, void *rhs, double dt,
 int cb_batch_run(cb_batch *b, int64_t nsteps);
 /* Steps taken and to take by a slot (host bookkeeping, no synchronisation). */
 int cb_batch_info(const cb_batch *b, int slot, int64_t *done, int64_t *target);
+/* Stage variant an admitted slot runs with: the variant selected for its
+ * (dim, N) when it was admitted, or 5 for the affine-element stage. */
+int cb_batch_slot_variant(const cb_batch *b, int slot, int *variant);
 /* Retire a slot: the instance's current state is placed in its Q (stream-
  * ordered), the twin buffer returns to the pool and the slot is free. */
 int cb_batch_release(cb_batch *b, int slot);

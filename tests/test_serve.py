@@ -4,8 +4,11 @@ served form stays within the precision-form tolerance of FP64, and admission
 respects the HBM budget.
 
 Tolerances: alone-vs-in-the-mix bit-identical; served FP64 vs one-at-a-time
-FP64 1e-13 relative L2 per field; served FP32 vs FP64 1e-5 per field for the
-inviscid requests and 1e-4 for the viscous ones (no state offsets there).
+FP64 1e-12 relative L2 per field (the oracle parity bar: the batch runs the
+vortex requests' affine meshes with the affine-element stage, whose geometry
+agrees with the per-node arrays of the one-at-a-time path to round-off);
+served FP32 vs FP64 1e-5 per field for the inviscid requests and 1e-4 for the
+viscous ones (no state offsets there).
 """
 import numpy as np
 import pytest
@@ -50,7 +53,7 @@ def test_served_fp64_equals_one_at_a_time_and_fp32_within_tolerance():
     served32 = _serve(reqs, 32)
     seq = S.serve_one_at_a_time(reqs, 64)
     for r in reqs:
-        assert max(relerr_fields(served64.results[r.rid], seq.results[r.rid])) < 1e-13, r.rid
+        assert max(relerr_fields(served64.results[r.rid], seq.results[r.rid])) < 1e-12, r.rid
         e32 = max(relerr_fields(served32.results[r.rid], seq.results[r.rid]))
         assert e32 < (1e-4 if r.kind == "ns3d" else 1e-5), (r.kind, e32)
 
