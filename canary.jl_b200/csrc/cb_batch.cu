@@ -45,16 +45,17 @@ __global__ void k_batch_step_end(BHdr *hdr) {
 }
 
 // Write the work items [pos, pos + ngroups) of the instance in `slot` into
-// list `sid` (groups of epb elements of nelem); when `d` is given, also its
-// descriptor, and reset its status word; set the list length to `count` when
-// count >= 0.
+// list `sid` (groups of epb elements of nelem); when `write` is set, also its
+// descriptor and gradient buffer `gq` (viscous batches), and reset its status
+// word; set the list length to `count` when count >= 0.
 template <typename T>
-__global__ void k_batch_admit(BHdr *hdr, int sid, int slot, BDesc<T> d, int write, int pos, int ngroups, int epb,
-                              int64_t nelem, int count) {
+__global__ void k_batch_admit(BHdr *hdr, int sid, int slot, BDesc<T> d, void *gq, int write, int pos, int ngroups,
+                              int epb, int64_t nelem, int count) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t == 0) {
     if (write) {
       static_cast<BDesc<T> *>(hdr->desc)[slot] = d;
+      if (hdr->gq) static_cast<void **>(hdr->gq)[slot] = gq;
       *d.status = 0;
     }
     if (count >= 0) hdr->nwork[sid] = count;
@@ -188,6 +189,8 @@ template <typename T>
 bool b_var_ok(int dim, int N, int var) {
   return b_order_ok(dim, N) && var >= 0 && var < NVAR_SEL && b_kernels<T>().fn[shape_id(dim, N, var)] != nullptr;
 }
+// viscous batches run the grouped two-pass LDG stage (variant 1 shapes)
+constexpr int VAR_VISC = 1;
 // default variant: the pipelined stage where it is built, else 512-node groups
 // (the autotuner may choose another)
 template <typename T>
@@ -208,6 +211,23 @@ cudaError_t b_prepare(int sid) {
     if (e != cudaSuccess) return e;
     k.grid[sid] = num_sms() * std::max(per_sm, 1);
     k.ready[sid] = true;
+  }
+  return cudaSuccess;
+}
+template <typename T>
+cudaError_t b_prepare_visc(int sid) {
+  BKernels<T> &k = b_kernels<T>();
+  if (!k.vready[sid]) {
+    for (int pass = 0; pass < 2; ++pass) {
+      cudaError_t e = cudaFuncSetAttribute(k.vfn[pass][sid], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)k.vsmem[pass][sid]);
+      if (e != cudaSuccess) return e;
+      int per_sm = 0;
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.vfn[pass][sid], BT, k.vsmem[pass][sid]);
+      if (e != cudaSuccess) return e;
+      k.vgrid[pass][sid] = num_sms() * std::max(per_sm, 1);
+    }
+    k.vready[sid] = true;
   }
   return cudaSuccess;
 }
@@ -241,7 +261,7 @@ struct BSlot {
   int64_t nelem = 0, start = 0, target = 0;
   int pos = 0, ngroups = 0;
   size_t qbytes = 0;
-  void *Q = nullptr, *alt = nullptr;
+  void *Q = nullptr, *alt = nullptr, *gq = nullptr;
   BDesc<double> d64{};  // template record of the instance (the batch's precision)
   BDesc<float> d32{};
 };
@@ -262,6 +282,8 @@ struct cb_batch {
   cb_phys phys{};
   unsigned *status = nullptr;  // per slot
   void *desc = nullptr;        // BDesc<T> per slot
+  void *gqtab = nullptr;       // viscous batches: gradient buffer per slot
+  bool visc = false;
   BHdr *hdr = nullptr;
   BList list[NSHAPE];
   std::vector<BSlot> slots;
@@ -291,7 +313,7 @@ BDesc<float> &record<float>(BSlot &s) { return s.d32; }
 template <typename T>
 cudaError_t launch_admit(cb_batch *b, int slot, const BSlot &sl, int pos, int count, bool write) {
   const int blocks = std::max(1, std::min(1024, (sl.ngroups + 255) / 256));
-  k_batch_admit<T><<<blocks, 256, 0, b->stream>>>(b->hdr, sl.sid, slot, record<T>(const_cast<BSlot &>(sl)),
+  k_batch_admit<T><<<blocks, 256, 0, b->stream>>>(b->hdr, sl.sid, slot, record<T>(const_cast<BSlot &>(sl)), sl.gq,
                                                   write ? 1 : 0, pos, sl.ngroups, sl.epb, sl.nelem, count);
   return cudaGetLastError();
 }
@@ -359,8 +381,29 @@ cudaError_t build_graph(cb_batch *b, const std::bitset<NSHAPE> &shapes) {
                 "BatchSrc layout");
   for (int sid = 0; sid < NSHAPE && e == cudaSuccess; ++sid) {
     if (!shapes.test(sid)) continue;
-    if ((e = b_prepare<T>(sid)) != cudaSuccess) break;
+    if ((e = b->visc ? b_prepare_visc<T>(sid) : b_prepare<T>(sid)) != cudaSuccess) break;
     cudaGraphNode_t prev = nullptr;
+    if (b->visc) {  // per stage: gradient pass, then the stage pass
+      for (int st = 0; st < 5 && e == cudaSuccess; ++st)
+        for (int pass = 0; pass < 2 && e == cudaSuccess; ++pass) {
+          int stage = st;
+          T rka = T(RKA[(st + 1) % 5]);
+          double rkb = RKB[st];
+          PhysT<T> pp = p;
+          void *gargs[] = {(void *)&hdr, (void *)&stage, (void *)&pp, (void *)&rka, (void *)&rkb};
+          cudaKernelNodeParams kp{};
+          kp.func = (void *)K.vfn[pass][sid];
+          kp.gridDim = dim3(K.vgrid[pass][sid]);
+          kp.blockDim = dim3(BT);
+          kp.sharedMemBytes = (unsigned)K.vsmem[pass][sid];
+          kp.kernelParams = gargs;
+          cudaGraphNode_t node;
+          e = cudaGraphAddKernelNode(&node, g, prev ? &prev : nullptr, prev ? 1 : 0, &kp);
+          prev = node;
+        }
+      if (e == cudaSuccess) lasts.push_back(prev);
+      continue;
+    }
     for (int st = 0; st < 5 && e == cudaSuccess; ++st) {
       int stage = st;
       T rka = T(RKA[(st + 1) % 5]);
@@ -437,20 +480,25 @@ int batch_add(cb_batch *b, const cb_mesh *m, void *Q, void *rhs, double dt, int6
   if (slot < 0) return solver_fail(CB_ERR_NOMEM, "cb_batch_add: all %d slots are in use", b->cap);
   const int Nq = m->N + 1, ns = m->dim == 2 ? 4 : 5;
   const int64_t Np = m->dim == 2 ? (int64_t)Nq * Nq : (int64_t)Nq * Nq * Nq;
-  const int var = b->var[m->dim - 2][m->N];
+  const int var = b->visc ? VAR_VISC : b->var[m->dim - 2][m->N];
   int sid = shape_id(m->dim, m->N, var);
   const BKernels<T> &K = b_kernels<T>();
-  const bool aff = b->affine && m->aff && b->phys.gravity == 0.0 && K.pipelined[sid] &&
+  const bool aff = !b->visc && b->affine && m->aff && b->phys.gravity == 0.0 && K.pipelined[sid] &&
                    K.fn[shape_id(m->dim, m->N, VAR_AFFINE)];
   if (aff) sid = shape_id(m->dim, m->N, VAR_AFFINE);
   const int epb = K.epb[sid];
   const int64_t ngroups = (m->nelem + epb - 1) / epb;
   const size_t qbytes = sizeof(T) * Np * ns * m->nelem;
-  void *alt = nullptr;
+  void *alt = nullptr, *gq = nullptr;
   cudaError_t e = cudaMallocFromPoolAsync(&alt, qbytes, b->pool, b->stream);
   if (e != cudaSuccess) return solver_fail(CB_ERR_NOMEM, "cb_batch_add: state twin: %s", cudaGetErrorString(e));
+  if (b->visc && (e = cudaMallocFromPoolAsync(&gq, qbytes * m->dim, b->pool, b->stream)) != cudaSuccess) {
+    cudaFreeAsync(alt, b->stream);
+    return solver_fail(CB_ERR_NOMEM, "cb_batch_add: gradient buffer: %s", cudaGetErrorString(e));
+  }
   if ((e = ensure_work<T>(b, sid, (int)ngroups)) != cudaSuccess) {
     cudaFreeAsync(alt, b->stream);
+    if (gq) cudaFreeAsync(gq, b->stream);
     return solver_fail(CB_ERR_NOMEM, "cb_batch_add: work list: %s", cudaGetErrorString(e));
   }
   BSlot sl;
@@ -467,6 +515,7 @@ int batch_add(cb_batch *b, const cb_mesh *m, void *Q, void *rhs, double dt, int6
   sl.qbytes = qbytes;
   sl.Q = Q;
   sl.alt = alt;
+  sl.gq = gq;
   BDesc<T> &d = record<T>(sl);
   d.Q[0] = (T *)Q;
   d.Q[1] = (T *)alt;
@@ -484,6 +533,7 @@ int batch_add(cb_batch *b, const cb_mesh *m, void *Q, void *rhs, double dt, int6
   sl.pos = L.tail;
   if ((e = launch_admit<T>(b, slot, sl, sl.pos, sl.pos + sl.ngroups, true)) != cudaSuccess) {
     cudaFreeAsync(alt, b->stream);
+    if (gq) cudaFreeAsync(gq, b->stream);
     return solver_fail(CB_ERR_CUDA, "cb_batch_add: %s", cudaGetErrorString(e));
   }
   L.tail = sl.pos + sl.ngroups;
@@ -509,6 +559,7 @@ int batch_release(cb_batch *b, int slot) {
     return solver_fail(CB_ERR_CUDA, "cb_batch_release: %s", cudaGetErrorString(e));
   L.tail = ntail;
   cudaFreeAsync(sl.alt, b->stream);
+  if (sl.gq) cudaFreeAsync(sl.gq, b->stream);
   sl = BSlot{};
   return CB_OK;
 }
@@ -636,15 +687,17 @@ int cb_batch_create(cb_batch **out, int precision, int max_instances, const cb_p
   if (precision != 32 && precision != 64) return solver_fail(CB_ERR_ARG, "precision must be 32 or 64");
   if (max_instances <= 0 || max_instances > (1 << 20))
     return solver_fail(CB_ERR_ARG, "cb_batch_create: max_instances must be 1..%d", 1 << 20);
-  if (phys->visc != 0.0) return solver_fail(CB_ERR_UNSUPPORTED, "the batched form is inviscid (visc must be 0)");
+  if (!(phys->visc >= 0.0)) return solver_fail(CB_ERR_ARG, "cb_batch_create: visc must be >= 0");
   cb_batch *b = new cb_batch();
   b->prec = precision;
   b->cap = max_instances;
   b->phys = *phys;
+  b->visc = phys->visc > 0.0;
   b->slots.resize(max_instances);
   for (int dim = 2; dim <= 3; ++dim)
     for (int N = 1; b_order_ok(dim, N); ++N)
-      b->var[dim - 2][N] = precision == 64 ? b_default_var<double>(dim, N) : b_default_var<float>(dim, N);
+      b->var[dim - 2][N] = b->visc ? VAR_VISC
+                                   : precision == 64 ? b_default_var<double>(dim, N) : b_default_var<float>(dim, N);
   cudaGetDevice(&b->device);
   cudaError_t e = cudaSuccess;
   auto bail = [&](const char *what) {
@@ -671,10 +724,12 @@ int cb_batch_create(cb_batch **out, int precision, int max_instances, const cb_p
   const size_t db = precision == 64 ? sizeof(BDesc<double>) : sizeof(BDesc<float>);
   if ((e = cudaMalloc((void **)&b->status, sizeof(unsigned) * max_instances)) != cudaSuccess ||
       (e = cudaMalloc((void **)&b->hdr, sizeof(BHdr))) != cudaSuccess ||
-      (e = cudaMalloc(&b->desc, db * max_instances)) != cudaSuccess)
+      (e = cudaMalloc(&b->desc, db * max_instances)) != cudaSuccess ||
+      (b->visc && (e = cudaMalloc(&b->gqtab, sizeof(void *) * max_instances)) != cudaSuccess))
     return bail("tables");
   BHdr h0{};
   h0.desc = b->desc;
+  h0.gq = b->gqtab;
   if ((e = cudaMemsetAsync(b->status, 0, sizeof(unsigned) * max_instances, b->stream)) != cudaSuccess ||
       (e = cudaMemsetAsync(b->desc, 0, db * max_instances, b->stream)) != cudaSuccess ||
       (e = cudaMemcpyAsync(b->hdr, &h0, sizeof h0, cudaMemcpyHostToDevice, b->stream)) != cudaSuccess ||
@@ -687,6 +742,8 @@ int cb_batch_create(cb_batch **out, int precision, int max_instances, const cb_p
 int cb_batch_set_variant(cb_batch *b, int dim, int N, int variant) {
   if (!b || (dim != 2 && dim != 3) || !b_order_ok(dim, N))
     return solver_fail(CB_ERR_ARG, "cb_batch_set_variant: bad arguments");
+  if (b->visc && variant != VAR_VISC)
+    return solver_fail(CB_ERR_UNSUPPORTED, "cb_batch_set_variant: viscous batches run variant %d only", VAR_VISC);
   if (!(b->prec == 64 ? b_var_ok<double>(dim, N, variant) : b_var_ok<float>(dim, N, variant)))
     return solver_fail(CB_ERR_UNSUPPORTED, "cb_batch_set_variant: variant %d is not built for dim %d N %d",
                        variant, dim, N);
@@ -764,13 +821,16 @@ int cb_batch_destroy(cb_batch *b) {
   if (!b) return CB_OK;
   if (b->stream) cudaStreamSynchronize(b->stream);
   drop_graph(b);
-  for (BSlot &s : b->slots)
+  for (BSlot &s : b->slots) {
     if (s.used && s.alt) cudaFreeAsync(s.alt, b->stream);
+    if (s.used && s.gq) cudaFreeAsync(s.gq, b->stream);
+  }
   for (BList &L : b->list)
     if (L.buf) cudaFreeAsync(L.buf, b->stream);
   if (b->stream) cudaStreamSynchronize(b->stream);
   cudaFree(b->status);
   cudaFree(b->desc);
+  cudaFree(b->gqtab);
   cudaFree(b->hdr);
   if (b->pool) cudaMemPoolDestroy(b->pool);
   if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);

@@ -74,6 +74,7 @@ struct BHdr {
   BWork *work[NSHAPE];
   int32_t nwork[NSHAPE];
   int64_t step;
+  void *gq;  // viscous batches: per slot the instance's gradient buffer (T *)
 };
 
 // One group of the fused stage (volume + face + LSRK update) of one instance.
@@ -222,6 +223,327 @@ k_stage_batch(const BHdr *__restrict__ hdr, int stage, PhysT<T> p, T rka, double
   }
 }
 
+// ---------------------------------------------------------------- viscous
+// LDG Navier–Stokes stage of a viscous batch, in two grouped passes per RK
+// stage instead of the reference's six (volume_grad!, flux_grad!,
+// update_gradQ!, volume_div!, flux_div!, updatesolution! with the inviscid
+// volumerhs!/fluxrhs!: nse3d.jl:475-955, nse2d.jl:396-778, nse2d.jl:1826-1849):
+//   grad:  gQ[:, s, c, e] = MJI (-Σ Dᵀ (MJ ξ_c prim_s) + Σ_f sMJ n_c avg_f prim_s)
+//          for the primitives (u, v, [w], ρ, T), written to the instance's
+//          gradient buffer (Np, nstate, dim, nelem);
+//   stage: the fused inviscid stage with the viscous flux folded in — flux
+//          rows MJ ξ·F_inv - μ MJ ξ·F_visc(gQ), face terms sMJ (Rusanov -
+//          μ n·(F_visc⁻ + F_visc⁺)/2) — then the LSRK update.
+// The viscous contributions are summed with the inviscid ones instead of in
+// a separate residual (the reference adds μ·rhs_gradQ at the update): the
+// same terms, rounded in another order.
+
+// Gradient pass of one group: gq of elements e0 .. e0 + nv - 1.
+template <int DIM, int Nq, typename T>
+__device__ __forceinline__ void ns_grad_group(const BDesc<T> &I, T *__restrict__ gq, int64_t e0, int nv, int par,
+                                              const PhysT<T> &p, unsigned char *smem) {
+  using C = BCfg<DIM, Nq, 0>;
+  constexpr int NS = Lay<DIM>::NS, NVG = Lay<DIM>::NVG, NSG = Lay<DIM>::NSG, IR = Lay<DIM>::IR, IE = Lay<DIM>::IE;
+  constexpr int Np = C::Np, Nfp = C::Nfp, NF = C::NFACE, SP = C::SLOTS, FS = C::EPB * Nfp, ND = NS * DIM;
+  constexpr int MJI = DIM * DIM + 1, GC = DIM * DIM + 2 + DIM - 1;
+  const T *__restrict__ Qin = I.Q[par];
+  const T *__restrict__ vgeo = I.vgeo;
+  T *Ds = reinterpret_cast<T *>(smem);
+  T *sQ = Ds + ((Nq * Nq + 1) & ~1);  // [NS][SP] state (offsets added)
+  T *sF = sQ + NS * SP;               // [DIM][NS][SP] rows of one gradient component
+  T *FF = sF + DIM * NS * SP;         // [NF][NS*DIM][FS] face terms sMJ n_c (prim⁻ + prim⁺)/2
+  for (int t = threadIdx.x; t < Nq * Nq; t += BT) Ds[t] = I.D[t];
+  T prim[C::NPT][NS], met[C::NPT][DIM][DIM], MJ[C::NPT];
+#pragma unroll
+  for (int u = 0; u < C::NPT; ++u) {
+    const int slot = threadIdx.x + u * BT;
+    const int el = slot / Np, n = slot % Np;
+    const int64_t e = e0 + el;
+    if (slot < SP && el < nv) {
+      T q[NS];
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        q[s] = Qin[n + Np * (s + NS * e)] + I.qref[s];
+        sQ[s * SP + slot] = q[s];
+      }
+      const T *vg = vgeo + (int64_t)Np * NVG * e;
+      load_metric<DIM, T>(vg, n, Np, met[u], MJ[u]);
+      const T gc = p.grav != T(0) ? vg[n + Np * GC] : T(0);
+      primitives<DIM, T>(q, gc, p, prim[u]);
+    }
+  }
+  __syncthreads();
+  // ---- face averages of the primitives (flux_grad!)
+  for (int fs = threadIdx.x; fs < C::FSLOTS; fs += BT) {
+    const int el = fs / (NF * Nfp), f = (fs / Nfp) % NF, fn = fs % Nfp;
+    if (el >= nv) continue;
+    const int64_t e = e0 + el;
+    const int vM = face_node<DIM, Nq>(f, fn);
+    const T *sg = I.sgeo + (int64_t)NSG * (fn + (int64_t)Nfp * (f + NF * e));
+    T nrm[DIM];
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) nrm[c] = sg[c];
+    const T sMJ = sg[DIM];
+    T qM[NS], pM[NS], pP[NS];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) qM[s] = sQ[s * SP + el * Np + vM];
+    const T gM = p.grav != T(0) ? vgeo[vM + Np * (GC + NVG * e)] : T(0);
+    primitives<DIM, T>(qM, gM, p, pM);
+    const int32_t nb = I.nbr[f + NF * e];
+    if (nb >= 0) {
+      const int64_t e2 = nb >> 3;
+      const int vP = face_node<DIM, Nq>(nb & 7, fn);
+      T qP[NS];
+#pragma unroll
+      for (int s = 0; s < NS; ++s) qP[s] = Qin[vP + Np * (s + NS * e2)] + I.qref[s];
+      const T gP = p.grav != T(0) ? vgeo[vP + Np * (GC + NVG * e2)] : T(0);
+      primitives<DIM, T>(qP, gP, p, pP);
+    } else {  // reflective wall: mirrored velocity, same density and temperature
+      T qP[NS];
+      wall_state<DIM, T>(qM, nrm, qP);
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) pP[c] = qP[c] / qM[IR];
+      pP[IR] = qM[IR];
+      pP[IE] = pM[IE];
+    }
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      const T fsv = T(0.5) * (pM[s] + pP[s]);
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) FF[(f * ND + s * DIM + c) * FS + el * Nfp + fn] = sMJ * nrm[c] * fsv;
+    }
+  }
+  // ---- per gradient component: volume term, face terms in face order, × MJI
+  for (int c = 0; c < DIM; ++c) {
+#pragma unroll
+    for (int u = 0; u < C::NPT; ++u) {
+      const int slot = threadIdx.x + u * BT;
+      const int el = slot / Np, n = slot % Np;
+      if (slot < SP && el < nv)
+#pragma unroll
+        for (int r = 0; r < DIM; ++r)
+#pragma unroll
+          for (int s = 0; s < NS; ++s) sF[(r * NS + s) * SP + el * Np + n] = MJ[u] * (met[u][r][c] * prim[u][s]);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < C::NPT; ++u) {
+      const int slot = threadIdx.x + u * BT;
+      const int el = slot / Np, n = slot % Np;
+      const int64_t e = e0 + el;
+      if (slot < SP && el < nv) {
+        T R[NS];
+#pragma unroll
+        for (int s = 0; s < NS; ++s) R[s] = T(0);
+        contract_sub<DIM, Nq, C::EPB, T>(sF, Ds, el, n, R);
+        const int i = n % Nq, j = (n / Nq) % Nq, k = DIM == 3 ? n / (Nq * Nq) : 0;
+        auto add = [&](int f, int fn) {
+#pragma unroll
+          for (int s = 0; s < NS; ++s) R[s] += FF[(f * ND + s * DIM + c) * FS + el * Nfp + fn];
+        };
+        if (i == 0) add(0, DIM == 3 ? j + Nq * k : j);
+        if (i == Nq - 1) add(1, DIM == 3 ? j + Nq * k : j);
+        if (j == 0) add(2, DIM == 3 ? i + Nq * k : i);
+        if (j == Nq - 1) add(3, DIM == 3 ? i + Nq * k : i);
+        if (DIM == 3 && k == 0) add(4, i + Nq * j);
+        if (DIM == 3 && k == Nq - 1) add(5, i + Nq * j);
+        const T mji = vgeo[n + Np * (MJI + (int64_t)NVG * e)];
+#pragma unroll
+        for (int s = 0; s < NS; ++s) gq[n + Np * (s + NS * (c + (int64_t)DIM * e))] = R[s] * mji;
+      }
+    }
+    __syncthreads();  // sF is rewritten for the next component; the last one frees shared memory
+  }
+}
+
+// Stage pass of one group: inviscid + viscous residual and the LSRK update.
+template <int DIM, int Nq, typename T>
+__device__ __forceinline__ void ns_stage_group(const BDesc<T> &I, const T *__restrict__ gq, int64_t e0, int nv,
+                                               int par, const PhysT<T> &p, T rka, T rkbdt, unsigned char *smem) {
+  using C = BCfg<DIM, Nq, 0>;
+  constexpr int NS = Lay<DIM>::NS, NVG = Lay<DIM>::NVG, NSG = Lay<DIM>::NSG, IR = Lay<DIM>::IR, IE = Lay<DIM>::IE;
+  constexpr int Np = C::Np, Nfp = C::Nfp, NF = C::NFACE, SP = C::SLOTS, FS = C::EPB * Nfp;
+  constexpr int MJI = DIM * DIM + 1, GC = DIM * DIM + 2 + DIM - 1;
+  const T *__restrict__ Qin = I.Q[par];
+  T *__restrict__ Qout = I.Q[par ^ 1];
+  T *__restrict__ rhs = I.rhs;
+  const T *__restrict__ vgeo = I.vgeo;
+  T *Ds = reinterpret_cast<T *>(smem);
+  T *sQ = Ds + ((Nq * Nq + 1) & ~1);  // [NS][SP] stored state (without offsets)
+  T *sF = sQ + NS * SP;               // [DIM][NS][SP], reused as the face buffer
+  for (int t = threadIdx.x; t < Nq * Nq; t += BT) Ds[t] = I.D[t];
+  T R[C::NPT][NS];
+#pragma unroll
+  for (int u = 0; u < C::NPT; ++u) {
+    const int slot = threadIdx.x + u * BT;
+    const int el = slot / Np, n = slot % Np;
+    const int64_t e = e0 + el;
+    if (slot < SP && el < nv) {
+      T q[NS];
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        const T d = Qin[n + Np * (s + NS * e)];
+        sQ[s * SP + slot] = d;
+        q[s] = d + I.qref[s];
+        R[u][s] = rhs[n + Np * (s + NS * e)];
+      }
+      const T *vg = vgeo + (int64_t)Np * NVG * e;
+      T met[DIM][DIM], MJ;
+      load_metric<DIM, T>(vg, n, Np, met, MJ);
+      const T gc = p.grav != T(0) ? vg[n + Np * GC] : T(0);
+      const T ri = T(1) / q[IR];
+      const T P = pressure_ri<DIM, T>(q, ri, gc, p);
+      T f[NS][DIM];
+      euler_flux_ri<DIM, T>(q, ri, P, f);
+      T g[NS][DIM], vel[DIM], fv[NS][DIM];
+#pragma unroll
+      for (int s = 0; s < NS; ++s)
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) g[s][c] = gq[n + Np * (s + NS * (c + (int64_t)DIM * e))];
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) vel[c] = q[c] / q[IR];
+      visc_flux<DIM, T>(g, vel, p, fv);
+#pragma unroll
+      for (int r = 0; r < DIM; ++r)
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+          T a = met[r][0] * f[s][0] + met[r][1] * f[s][1];
+          T b = met[r][0] * fv[s][0] + met[r][1] * fv[s][1];
+          if (DIM == 3) {
+            a = a + met[r][2] * f[s][2];
+            b = b + met[r][2] * fv[s][2];
+          }
+          sF[(r * NS + s) * SP + el * Np + n] = MJ * a - p.visc * (MJ * b);
+        }
+      R[u][DIM - 1] -= MJ * q[IR] * p.grav;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int u = 0; u < C::NPT; ++u) {
+    const int slot = threadIdx.x + u * BT;
+    const int el = slot / Np, n = slot % Np;
+    if (slot < SP && el < nv) contract<DIM, Nq, C::EPB, T>(sF, Ds, el, n, R[u]);
+  }
+  __syncthreads();
+  // ---- face terms into FF[NF][NS][EPB*Nfp] (aliases sF): Rusanov - μ viscous average
+  T *FF = sF;
+  for (int fs = threadIdx.x; fs < C::FSLOTS; fs += BT) {
+    const int el = fs / (NF * Nfp), f = (fs / Nfp) % NF, fn = fs % Nfp;
+    if (el >= nv) continue;
+    const int64_t e = e0 + el;
+    const int vM = face_node<DIM, Nq>(f, fn);
+    const T *sg = I.sgeo + (int64_t)NSG * (fn + (int64_t)Nfp * (f + NF * e));
+    T nrm[DIM];
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) nrm[c] = sg[c];
+    const T smj = sg[DIM];
+    T qM[NS], qP[NS], gm[NS][DIM], gp[NS][DIM], vM_[DIM], vP_[DIM];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) qM[s] = sQ[s * SP + el * Np + vM] + I.qref[s];
+#pragma unroll
+    for (int s = 0; s < NS; ++s)
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) gm[s][c] = gq[vM + Np * (s + NS * (c + (int64_t)DIM * e))];
+    const T gM = p.grav != T(0) ? vgeo[vM + Np * (GC + NVG * e)] : T(0);
+    const T riM = T(1) / qM[IR];
+    const T PM = pressure_ri<DIM, T>(qM, riM, gM, p);
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) vM_[c] = qM[c] / qM[IR];
+    const int32_t nb = I.nbr[f + NF * e];
+    T PP, riP;
+    if (nb >= 0) {
+      const int64_t e2 = nb >> 3;
+      const int vP = face_node<DIM, Nq>(nb & 7, fn);
+#pragma unroll
+      for (int s = 0; s < NS; ++s) qP[s] = Qin[vP + Np * (s + NS * e2)] + I.qref[s];
+#pragma unroll
+      for (int s = 0; s < NS; ++s)
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) gp[s][c] = gq[vP + Np * (s + NS * (c + (int64_t)DIM * e2))];
+      const T gP = p.grav != T(0) ? vgeo[vP + Np * (GC + NVG * e2)] : T(0);
+      riP = T(1) / qP[IR];
+      PP = pressure_ri<DIM, T>(qP, riP, gP, p);
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) vP_[c] = qP[c] / qP[IR];
+    } else {  // reflective wall (nse3d.jl:880-900): mirrored state, velocity and gradients
+      wall_state<DIM, T>(qM, nrm, qP);
+      riP = riM;
+      PP = PM;
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        T sn = nrm[0] * gm[s][0] + nrm[1] * gm[s][1];
+        if (DIM == 3) sn = sn + nrm[2] * gm[s][2];
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) gp[s][c] = gm[s][c] - T(2) * sn * nrm[c];
+      }
+      T un = nrm[0] * vM_[0] + nrm[1] * vM_[1];
+      if (DIM == 3) un = un + nrm[2] * vM_[2];
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) vP_[c] = vM_[c] - T(2) * un * nrm[c];
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) gp[IE][c] = gm[IE][c];
+    }
+    T out[NS];
+    rusanov_n<DIM, T>(qM, riM, PM, qP, riP, PP, nrm, p, out);
+    T fM[NS][DIM], fP[NS][DIM];
+    visc_flux<DIM, T>(gm, vM_, p, fM);
+    visc_flux<DIM, T>(gp, vP_, p, fP);
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      T a = nrm[0] * (fM[s][0] + fP[s][0]) + nrm[1] * (fM[s][1] + fP[s][1]);
+      if (DIM == 3) a = a + nrm[2] * (fM[s][2] + fP[s][2]);
+      FF[(f * NS + s) * FS + el * Nfp + fn] = smj * out[s] - p.visc * (smj * (T(0.5) * a));
+    }
+  }
+  __syncthreads();
+  bool bad = false;
+#pragma unroll
+  for (int u = 0; u < C::NPT; ++u) {
+    const int slot = threadIdx.x + u * BT;
+    const int el = slot / Np, n = slot % Np;
+    const int64_t e = e0 + el;
+    if (slot < SP && el < nv) {
+      gather_face_terms<DIM, Nq, C::EPB, T>(FF, el, n, R[u]);
+      const T mji = vgeo[n + Np * (MJI + (int64_t)NVG * e)];
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        const T qn = sQ[s * SP + slot] + rkbdt * R[u][s] * mji;
+        bad |= !isfinite(qn);
+        Qout[n + Np * (s + NS * e)] = qn;
+        rhs[n + Np * (s + NS * e)] = R[u][s] * rka;
+      }
+    }
+  }
+  if (bad) atomicOr(I.status, ST_NONFINITE);
+  __syncthreads();  // shared memory is reused by the block's next item
+}
+
+// Persistent viscous passes of one shape (the grouped variant's work list).
+template <int DIM, int Nq, typename T, bool GRAD>
+__global__ void __launch_bounds__(BT, 1)
+k_ns_batch(const BHdr *__restrict__ hdr, int stage, PhysT<T> p, T rka, double rkb) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int SID = shape_id(DIM, Nq - 1, 1);
+  const int nwork = hdr->nwork[SID];
+  const int64_t step = hdr->step;
+  const BWork *__restrict__ work = hdr->work[SID];
+  const BDesc<T> *__restrict__ desc = static_cast<const BDesc<T> *>(hdr->desc);
+  T *const *gqt = static_cast<T *const *>(hdr->gq);
+  for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+    const BWork it = work[w];
+    if (!it.valid) continue;  // uniform over the block
+    const BDesc<T> &I = desc[it.slot];
+    const int64_t k = step - I.start;
+    if (k >= I.target) continue;
+    const int par = (int)((k + stage) & 1);
+    if constexpr (GRAD)
+      ns_grad_group<DIM, Nq, T>(I, gqt[it.slot], it.e0, it.nv, par, p, smem_raw);
+    else
+      ns_stage_group<DIM, Nq, T>(I, gqt[it.slot], it.e0, it.nv, par, p, rka, T(rkb * I.dt), smem_raw);
+  }
+}
+
 // Item source of the pipelined stage over a work list of many instances
 // (see k_stage_pipe2).  The second warp of the block (the first issues the
 // bulk copies) finds the block's next live item and publishes it into a
@@ -348,6 +670,11 @@ struct BKernels {
   int epb[NSHAPE] = {}, threads[NSHAPE] = {}, grid[NSHAPE] = {};
   size_t smem[NSHAPE] = {};
   bool pipelined[NSHAPE] = {}, ready[NSHAPE] = {};
+  // viscous batches (variant 1 shapes only): gradient and stage passes
+  const void *vfn[2][NSHAPE] = {};
+  int vgrid[2][NSHAPE] = {};
+  size_t vsmem[2][NSHAPE] = {};
+  bool vready[NSHAPE] = {};
 };
 template <int DIM, int Nq, int G, typename T>
 constexpr size_t b_group_smem() {
@@ -394,6 +721,15 @@ void b_fill(BKernels<T> &k) {
     k.epb[id] = BCfg<DIM, Nq, 1>::EPB;
     k.threads[id] = BT;
     k.smem[id] = b_group_smem<DIM, Nq, 1, T>();
+  }
+  {
+    using C = BCfg<DIM, Nq, 0>;
+    const int id = shape_id(DIM, N, 1);
+    k.vfn[0][id] = (const void *)k_ns_batch<DIM, Nq, T, true>;
+    k.vfn[1][id] = (const void *)k_ns_batch<DIM, Nq, T, false>;
+    k.vsmem[0][id] = b_group_smem<DIM, Nq, 0, T>() +
+                     sizeof(T) * (size_t)C::NFACE * Lay<DIM>::NS * DIM * C::EPB * C::Nfp;
+    k.vsmem[1][id] = b_group_smem<DIM, Nq, 0, T>();
   }
 }
 // Fill the table entries of one dimension (one translation unit per

@@ -215,7 +215,9 @@ int cb_computegeometry(int dim, int N, int64_t nelem, const double *elemtocoord,
  * of uneven order and element count together, each with its own dt, step
  * count and state, with the same per-instance result as cb_lsrk_run (the
  * fused stage arithmetic is the same; results do not depend on what else is
- * in the batch).  Inviscid form, dim 2 with N 1..8 and dim 3 with N 1..7.
+ * in the batch).  Dim 2 with N 1..8 and dim 3 with N 1..7; Euler, or LDG
+ * Navier-Stokes when the batch's visc > 0 (nse2d.jl / nse3d.jl viscous
+ * passes, as cb_lsrk_run with visc > 0, fused into two passes per stage).
  *
  * A cb_mesh holds what instances on the same mesh share: the geometry (the
  * caller's FP64 arrays for precision 64, rounded FP32 copies for precision 32)
@@ -239,7 +241,10 @@ int cb_mesh_destroy(cb_mesh *m);
 
 /* A batch of up to max_instances slots.  All calls are ordered on `stream`
  * (0: the batch makes its own) and asynchronous except cb_batch_status and
- * cb_batch_destroy.  visc must be 0. */
+ * cb_batch_destroy.  visc >= 0; with visc > 0 every instance is advanced by
+ * the LDG Navier-Stokes stage (a gradient pass writing a batch-owned
+ * (Np, nstate, dim, nelem) buffer per instance, then the fused inviscid +
+ * viscous stage), variant 1 only. */
 typedef struct cb_batch cb_batch;
 int cb_batch_create(cb_batch **out, int precision, int max_instances,
                     const cb_phys *phys, cb_stream_t stream);

@@ -63,7 +63,7 @@ def test_check_raises():
 def test_batch_argument_validation_without_device():
     L = _lib.lib()
     phys = _lib.cb_phys(1.4, 1.0, 3.5, 2.5, 0.0, 0.72, -2 / 3, 0.0)
-    visc = _lib.cb_phys(1.4, 1.0, 3.5, 2.5, 0.0, 0.72, -2 / 3, 1e-3)
+    negvisc = _lib.cb_phys(1.4, 1.0, 3.5, 2.5, 0.0, 0.72, -2 / 3, -1e-3)
     dummy = C.c_void_p(16)
     h = C.c_void_p()
     # orders outside the batched range, bad dim / precision, null arrays
@@ -79,8 +79,8 @@ def test_batch_argument_validation_without_device():
                             None) == _lib.CB_ERR_ARG
     assert L.cb_batch_create(C.byref(h), 16, 8, C.byref(phys), None) == _lib.CB_ERR_ARG
     assert L.cb_batch_create(C.byref(h), 64, 0, C.byref(phys), None) == _lib.CB_ERR_ARG
-    assert L.cb_batch_create(C.byref(h), 64, 8, C.byref(visc), None) == _lib.CB_ERR_UNSUPPORTED
-    assert "inviscid" in L.cb_last_error().decode()
+    assert L.cb_batch_create(C.byref(h), 64, 8, C.byref(negvisc), None) == _lib.CB_ERR_ARG
+    assert "visc" in L.cb_last_error().decode()
     assert L.cb_batch_set_variant(None, 2, 3, 0) == _lib.CB_ERR_ARG
     assert L.cb_batch_run(None, 1) == _lib.CB_ERR_ARG
     assert L.cb_batch_release(None, 0) == _lib.CB_ERR_ARG
