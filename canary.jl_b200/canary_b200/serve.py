@@ -6,8 +6,9 @@ size, its initial-condition parameters and a final time.  The server keeps
 every admitted state resident on the device, admits requests in arrival order
 while their memory fits an HBM budget, and advances all inviscid requests
 together in one Batch (one graph launch per LSRK step, each instance with its
-own dt and step count).  Viscous requests run as their own solver on a side
-stream, overlapping the batch on the device.  Finished instances are retired
+own dt and step count) and all Navier–Stokes requests in a second, viscous
+Batch on its own stream, overlapping the first on the device.  Finished
+instances are retired
 and copied to pinned host memory without stopping the others, and their slots
 and memory go to the next requests.  Latency is arrival -> final state on the
 host, timed with CUDA events on the device clock.
@@ -111,7 +112,9 @@ class MeshPool:
         b32 = 4 * nelem * (Np * nvg + nsg * Nfp * 2 * dim + 2 * dim)
         return b64 + (b32 if precision == 32 else 0)
 
-    def get(self, req: Request, precision: int):
+    def get(self, req: Request, precision: int, batch: bool = True):
+        """The request's mesh; with `batch`, also its batch mesh (cb_mesh) of
+        that precision."""
         torch = _torch()
         k = self.key(req)
         m = self.meshes.get(k)
@@ -123,7 +126,7 @@ class MeshPool:
                                       warp_amp=0.0 if req.dim == 2 else 0.05, device=self.device,
                                       stream=self.stream)
             m = self.meshes[k] = _Mesh(dm, self.nbytes(req.dim, req.N, req.n_side, precision))
-        if precision not in m.batch and req.kind != "ns3d":
+        if batch and precision not in m.batch:
             m.batch[precision] = BatchMesh(m.dmesh, precision, stream=self.stream)
         m.users += 1
         m.last = time.perf_counter()
@@ -148,6 +151,17 @@ class MeshPool:
         return True
 
 
+class _Lane:
+    """One batch (inviscid or viscous) with its stream and the asynchronous
+    copy of its per-slot status words."""
+
+    def __init__(self, batch: Batch, stream, max_instances: int):
+        torch = _torch()
+        self.batch, self.stream = batch, stream
+        self.stat = torch.zeros(max_instances, dtype=torch.int32, pin_memory=True)
+        self.stat_ev, self.stat_tick, self.live = None, 0, 0
+
+
 @dataclass
 class _Live:
     req: Request
@@ -156,17 +170,14 @@ class _Live:
     dt: float
     bytes: int
     offset: np.ndarray
+    lane: _Lane = None
     Q: object = None
     rhs: object = None
     slot: int = -1
-    solver: object = None
-    stream: object = None
     left: int = 0
     admitted: float = 0.0
     failed: bool = False
     tick0: int = 0  # loop tick at admission
-    stat: object = None  # pinned status word (viscous solver)
-    stat_ev: object = None
 
 
 @dataclass
@@ -216,8 +227,7 @@ class Server:
     state offsets); tick_steps steps are launched per loop iteration, with at
     most two ticks in flight."""
 
-    def __init__(self, precision=32, hbm_budget=120e9, max_instances=4096, tick_steps=8, device="cuda",
-                 viscous_streams=8):
+    def __init__(self, precision=32, hbm_budget=120e9, max_instances=4096, tick_steps=8, device="cuda"):
         torch = _torch()
         self.torch = torch
         self.device = torch.device(device)
@@ -225,14 +235,16 @@ class Server:
         self.real = torch.float32 if precision == 32 else torch.float64
         self.budget = int(hbm_budget)
         self.tick = tick_steps
-        self.bstream = torch.cuda.Stream(self.device)  # batch and its admissions / retirements
         self.sstream = torch.cuda.Stream(self.device)  # meshes and initial states
-        # viscous requests: one solver each, spread over a few streams so that
-        # small solves run concurrently
-        self.vstreams = [torch.cuda.Stream(self.device) for _ in range(viscous_streams)]
-        self.batch = Batch(precision, max_instances, make_phys(), stream=self.bstream)
         self.max_instances = max_instances
-        self.vphys = make_phys(visc=VISC)
+        # the inviscid and the viscous batch, each on its own stream (with
+        # their admissions and retirements)
+        self.lanes = {}
+        for visc in (False, True):
+            st = torch.cuda.Stream(self.device)
+            phys = make_phys(visc=VISC) if visc else make_phys()
+            self.lanes[visc] = _Lane(Batch(precision, max_instances, phys, stream=st), st, max_instances)
+        self.batch = self.lanes[False].batch
         self.pool = MeshPool(self.device, self.sstream)
         self.in_use = 0
 
@@ -241,8 +253,8 @@ class Server:
         Nq = req.N + 1
         n = (req.n_side ** req.dim) * (Nq ** req.dim) * nstate(req.dim)
         w = 4 if self.precision == 32 else 8
-        if req.kind == "ns3d":  # Q, rhs, gradQ, rhs_gradQ (dim x state each), FP32 geometry copy
-            return w * n * (2 + 2 * req.dim) + (MeshPool.nbytes(3, req.N, req.n_side, 32) // 2)
+        if req.kind == "ns3d":  # Q, rhs, batch-owned twin and gradient (dim x state)
+            return w * n * (3 + req.dim)
         return 3 * w * n  # Q, rhs, batch-owned twin
 
     def _initial(self, req: Request, m: _Mesh):
@@ -255,7 +267,7 @@ class Server:
             f = ic.fourier_state_t(x[0], x[1], x[2], seed=req.seed)
             off = np.array([0.0, 0.0, 0.0, 1.0, 1.0 / (GAMMA - 1.0)])
         speed = float(wave_speed(f, req.dim).item())  # synchronises the setup stream only
-        if self.precision == 64 or req.kind == "ns3d":
+        if self.precision == 64:
             off = np.zeros(nstate(req.dim))
         Q = ic.device_state(list(f), self.real, off)
         return Q, torch.zeros_like(Q), off, speed
@@ -266,20 +278,13 @@ class Server:
         with torch.cuda.stream(self.sstream):
             Q, rhs, off, speed = self._initial(req, m)
         nsteps, dt = plan(req, speed)
-        live = _Live(req, m, nsteps, dt, self.request_bytes(req), off, Q, rhs, left=nsteps, admitted=now)
-        if req.kind == "ns3d":
-            vs = self.vstreams[req.rid % len(self.vstreams)]
-            live.stream = vs
-            vs.wait_stream(self.sstream)
-            Q.record_stream(vs)
-            rhs.record_stream(vs)
-            live.solver = LSRK(m.dmesh, Q, rhs, self.precision, self.vphys, stream=vs)
-            live.stat = torch.zeros(1, dtype=torch.int32, pin_memory=True)
-        else:
-            self.bstream.wait_stream(self.sstream)
-            Q.record_stream(self.bstream)
-            rhs.record_stream(self.bstream)
-            live.slot = self.batch.add(m.batch[self.precision], Q, rhs, dt, nsteps, off)
+        lane = self.lanes[req.kind == "ns3d"]
+        live = _Live(req, m, nsteps, dt, self.request_bytes(req), off, lane, Q, rhs, left=nsteps, admitted=now)
+        lane.stream.wait_stream(self.sstream)
+        Q.record_stream(lane.stream)
+        rhs.record_stream(lane.stream)
+        live.slot = lane.batch.add(m.batch[self.precision], Q, rhs, dt, nsteps, off)
+        lane.live += 1
         self.in_use += live.bytes
         return live
 
@@ -298,12 +303,11 @@ class Server:
         waiting, live, retiring = deque(), {}, []
         lat, results, failed = {}, {}, set()
         flight = {}  # stream -> events of the ticks in flight
-        bstat = torch.zeros(self.max_instances, dtype=torch.int32, pin_memory=True)
-        bstat_ev, bstat_tick, ticks = None, 0, 0
+        ticks = 0
         dof_stage, peak, max_live = 0.0, 0, 0
         base = torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize(self.device)
-        base.record(self.bstream)
+        base.record(self.lanes[False].stream)
         t0 = time.perf_counter()
 
         def tick_done(stream):
@@ -328,60 +332,44 @@ class Server:
             peak = max(peak, self.in_use + self.pool.resident_bytes())
             max_live = max(max_live, len(live))
             # non-finite states (status copied after an earlier tick): retire early as failed
-            if bstat_ev is not None and bstat_ev.query():
-                bits = bstat.numpy()
-                for lv in live.values():
-                    # a slot's word is reset at admission: only instances admitted
-                    # before the copied tick are described by it
-                    if lv.solver is None and lv.tick0 < bstat_tick and bits[lv.slot] & 2:
-                        lv.failed = True
-                bstat_ev = None
-            for lv in live.values():
-                if lv.solver is not None and lv.stat_ev is not None and lv.stat_ev.query():
-                    lv.failed = bool(int(lv.stat[0]) & 2)
-                    lv.stat_ev = None
+            for lane in self.lanes.values():
+                if lane.stat_ev is not None and lane.stat_ev.query():
+                    bits = lane.stat.numpy()
+                    for lv in live.values():
+                        # a slot's word is reset at admission: only instances admitted
+                        # before the copied tick are described by it
+                        if lv.lane is lane and lv.tick0 < lane.stat_tick and bits[lv.slot] & 2:
+                            lv.failed = True
+                    lane.stat_ev = None
             if live:
-                # one tick: K batch steps and K steps of every viscous solver
-                self.batch.run(self.tick)
-                used = set()
+                # one tick: K steps of both batches (concurrent streams)
+                for lane in self.lanes.values():
+                    if lane.live:
+                        lane.batch.run(self.tick)
                 for rid, lv in list(live.items()):
                     Nq = lv.req.N + 1
                     dofs = nstate(lv.req.dim) * (lv.req.n_side ** lv.req.dim) * Nq ** lv.req.dim
-                    if lv.solver is None:
-                        done, target = self.batch.info(lv.slot)
-                        dof_stage += 5 * dofs * (lv.left - (target - done))
-                        lv.left = target - done
-                    elif not lv.failed:
-                        k = min(self.tick, lv.left)
-                        lv.solver.run(k, lv.dt)
-                        lv.left -= k
-                        dof_stage += 5 * dofs * k
-                        used.add(lv.stream)
-                        if lv.stat_ev is None and lv.left > 0:
-                            lv.solver.status_async(lv.stat)
-                            lv.stat_ev = torch.cuda.Event()
-                            lv.stat_ev.record(lv.stream)
+                    done, target = lv.lane.batch.info(lv.slot)
+                    dof_stage += 5 * dofs * (lv.left - (target - done))
+                    lv.left = target - done
                     if lv.left <= 0 or lv.failed:
                         if lv.failed:
                             failed.add(rid)
                         retiring.append(self._retire(lv))
                         del live[rid]
                 ticks += 1
-                if bstat_ev is None:
-                    self.batch.status_async(bstat)
-                    bstat_ev = torch.cuda.Event()
-                    bstat_ev.record(self.bstream)
-                    bstat_tick = ticks
-                tick_done(self.bstream)
-                for vs in used:
-                    tick_done(vs)
+                for lane in self.lanes.values():
+                    if lane.stat_ev is None and lane.live:
+                        lane.batch.status_async(lane.stat)
+                        lane.stat_ev = torch.cuda.Event()
+                        lane.stat_ev.record(lane.stream)
+                        lane.stat_tick = ticks
+                    tick_done(lane.stream)
             elif reqs and realtime:
                 time.sleep(max(0.0, min(reqs[0].arrival - (time.perf_counter() - t0), 0.002)))
             for item in list(retiring):
                 ev, lv, host = item
                 if ev.query():
-                    if lv.solver is not None:
-                        lv.solver.close()
                     lat[lv.req.rid] = base.elapsed_time(ev) * 1e-3 - (lv.req.arrival if realtime else 0.0)
                     results[lv.req.rid] = host.numpy().reshape(
                         (lv.req.n_side ** lv.req.dim, nstate(lv.req.dim), (lv.req.N + 1) ** lv.req.dim)
@@ -401,11 +389,9 @@ class Server:
 
     def _retire(self, lv: _Live):
         torch = self.torch
-        if lv.solver is not None:
-            stream = lv.stream  # the solver is closed once its copy-out has completed
-        else:
-            self.batch.release(lv.slot)  # places the final state in lv.Q (stream-ordered)
-            stream = self.bstream
+        lv.lane.batch.release(lv.slot)  # places the final state in lv.Q (stream-ordered)
+        lv.lane.live -= 1
+        stream = lv.lane.stream
         host = torch.empty(lv.Q.numel(), dtype=torch.float64, pin_memory=True)
         with torch.cuda.stream(stream):
             host.copy_(lv.Q, non_blocking=True) if lv.Q.dtype == torch.float64 else \
@@ -415,7 +401,8 @@ class Server:
         return (ev, lv, host)
 
     def close(self):
-        self.batch.close()
+        for lane in self.lanes.values():
+            lane.batch.close()
         for m in self.pool.meshes.values():
             for bm in m.batch.values():
                 bm.close()
@@ -440,7 +427,7 @@ def serve_one_at_a_time(requests, precision=64, device="cuda"):
     for r in sorted(requests, key=lambda q: (q.arrival, q.rid)):
         while time.perf_counter() - t0 < r.arrival:
             time.sleep(min(0.002, r.arrival - (time.perf_counter() - t0)))
-        m = pool.get(r, precision)
+        m = pool.get(r, precision, batch=False)
         x = m.dmesh.coords()
         with torch.cuda.stream(stream):
             if r.kind == "vortex":
