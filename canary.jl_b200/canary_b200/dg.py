@@ -44,6 +44,14 @@ def nstate(dim: int) -> int:
     return 5 if dim == 3 else 4
 
 
+def viscous_fused(dim: int, N: int) -> bool:
+    """Whether the viscous solver of (dim, N) runs the two fused passes per
+    stage (element groups of at most two nodes per thread of a 256-thread
+    block: every 2-D order, 3-D up to N = 7) and so takes state offsets; other
+    orders run the reference's unfused pass sequence."""
+    return dim == 2 or (N + 1) ** 3 <= 512
+
+
 def _torch():
     import torch
     return torch

@@ -544,6 +544,31 @@ k_ns_batch(const BHdr *__restrict__ hdr, int stage, PhysT<T> p, T rka, double rk
   }
 }
 
+// The two viscous passes over one mesh (cb_lsrk_run with visc > 0): groups
+// of BCfg<DIM, Nq, 0>::EPB consecutive elements, blocks striding over them;
+// the state is read from I.Q[0] and written to I.Q[1].
+template <int DIM, int Nq, typename T, bool GRAD>
+__global__ void __launch_bounds__(BT, 1)
+k_ns_mesh(BDesc<T> I, T *gq, int64_t nelem, PhysT<T> p, T rka, T rkbdt) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int EPB = BCfg<DIM, Nq, 0>::EPB;
+  for (int64_t g = blockIdx.x; g * EPB < nelem; g += gridDim.x) {
+    const int64_t e0 = g * EPB;
+    const int nv = nelem - e0 < EPB ? (int)(nelem - e0) : EPB;
+    if constexpr (GRAD)
+      ns_grad_group<DIM, Nq, T>(I, gq, e0, nv, 0, p, smem_raw);
+    else
+      ns_stage_group<DIM, Nq, T>(I, gq, e0, nv, 0, p, rka, rkbdt, smem_raw);
+  }
+}
+// Shared memory of the gradient (pass 0) and stage (pass 1) passes.
+template <int DIM, int Nq, typename T>
+constexpr size_t ns_smem(int pass) {
+  using C = BCfg<DIM, Nq, 0>;
+  return sizeof(T) * (((Nq * Nq + 1) & ~1) + (size_t)Lay<DIM>::NS * C::SLOTS + (size_t)DIM * Lay<DIM>::NS * C::SLOTS +
+                      (pass == 0 ? (size_t)C::NFACE * Lay<DIM>::NS * DIM * C::EPB * C::Nfp : 0));
+}
+
 // Item source of the pipelined stage over a work list of many instances
 // (see k_stage_pipe2).  The second warp of the block (the first issues the
 // bulk copies) finds the block's next live item and publishes it into a
@@ -723,13 +748,11 @@ void b_fill(BKernels<T> &k) {
     k.smem[id] = b_group_smem<DIM, Nq, 1, T>();
   }
   {
-    using C = BCfg<DIM, Nq, 0>;
     const int id = shape_id(DIM, N, 1);
     k.vfn[0][id] = (const void *)k_ns_batch<DIM, Nq, T, true>;
     k.vfn[1][id] = (const void *)k_ns_batch<DIM, Nq, T, false>;
-    k.vsmem[0][id] = b_group_smem<DIM, Nq, 0, T>() +
-                     sizeof(T) * (size_t)C::NFACE * Lay<DIM>::NS * DIM * C::EPB * C::Nfp;
-    k.vsmem[1][id] = b_group_smem<DIM, Nq, 0, T>();
+    k.vsmem[0][id] = ns_smem<DIM, Nq, T>(0);
+    k.vsmem[1][id] = ns_smem<DIM, Nq, T>(1);
   }
 }
 // Fill the table entries of one dimension (one translation unit per

@@ -7,6 +7,9 @@ namespace cb {
 constexpr int MAXN = 10;  // orders 1..MAXN are compiled for dim 2 and 3
 
 template <typename T>
+struct BDesc;
+
+template <typename T>
 struct Ops {
   int Np, Nfp, epb, threads;
   size_t smem_stage;
@@ -31,6 +34,9 @@ struct Ops {
   cudaError_t (*update_gradQ)(T *, const T *, const T *, int64_t, int, cudaStream_t);
   cudaError_t (*cons_sums)(const T *, const T *, int64_t, int, const Offs<double, 5> &, double *, int,
                            cudaStream_t);
+  // fused viscous passes over one mesh (pass 0: gradient, 1: stage + update);
+  // nullptr for orders whose groups would need more than two nodes per thread
+  cudaError_t (*ns_pass)(int, const BDesc<T> &, T *, int64_t, const PhysT<T> &, T, T, cudaStream_t);
 };
 
 // Defined in cb_inst_<dim>d_<prec>.cu; nullptr when N is outside 1..MAXN.

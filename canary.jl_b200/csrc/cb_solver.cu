@@ -6,9 +6,11 @@
 // and a solver-owned twin.  Two steps (ten stages) return to the caller's
 // buffer and are captured as one CUDA graph; an odd final step is launched
 // directly and copied back.
-// Viscous (LDG Navier–Stokes) form: the reference sequence of passes per
-// stage (volume, face, gradient, divergence, update) on a single buffer,
-// captured one step per graph.
+// Viscous (LDG Navier–Stokes) form: for orders whose element groups fit two
+// nodes per thread, two fused passes per stage (gradient, then inviscid +
+// viscous residual and update) that ping-pong like the inviscid form; above
+// that, the reference sequence of passes per stage (volume, face, gradient,
+// divergence, update) on a single buffer, captured one step per graph.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -17,6 +19,7 @@
 #include <string>
 
 #include "../../include/canary_b200.h"
+#include "cb_batch.cuh"
 #include "cb_ops.h"
 
 using namespace cb;
@@ -58,6 +61,12 @@ template <typename T>
 const Ops<T> *ops(const cb_solver *s) {
   return s->dim == 2 ? get_ops<2, T>(s->N) : get_ops<3, T>(s->N);
 }
+// viscous form through the two fused passes
+bool fused_visc(const cb_solver *s) {
+  return s->phys.visc > 0 && (s->prec == 64 ? ops<double>(s)->ns_pass != nullptr : ops<float>(s)->ns_pass != nullptr);
+}
+// the state ping-pongs between Q and Qalt (two steps per graph)
+bool pingpong(const cb_solver *s) { return s->phys.visc <= 0 || fused_visc(s); }
 
 template <typename T>
 cudaError_t enqueue_step(cb_solver *s, double dt, bool from_user) {
@@ -66,6 +75,28 @@ cudaError_t enqueue_step(cb_solver *s, double dt, bool from_user) {
                         s->phys.Pr, s->phys.lambda, s->phys.visc});
   const T *vg = (const T *)s->vgeo, *sg = (const T *)s->sgeo, *D = (const T *)s->D;
   cudaError_t e = cudaSuccess;
+  if (fused_visc(s)) {
+    T *a = (T *)(from_user ? s->Q : s->Qalt), *b = (T *)(from_user ? s->Qalt : s->Q);
+    BDesc<T> I{};
+    I.rhs = (T *)s->rhs;
+    I.vgeo = vg;
+    I.sgeo = sg;
+    I.D = D;
+    I.nbr = s->nbr;
+    I.status = s->status;
+    I.dt = dt;
+    for (int k = 0; k < 5; ++k) I.qref[k] = T(s->qref[k]);
+    for (int st = 0; st < 5 && e == cudaSuccess; ++st) {
+      I.Q[0] = a;
+      I.Q[1] = b;
+      if ((e = o->ns_pass(0, I, (T *)s->gradQ, s->nelem, p, T(0), T(0), s->stream)) != cudaSuccess) break;
+      e = o->ns_pass(1, I, (T *)s->gradQ, s->nelem, p, T(RKA[(st + 1) % 5]), T(RKB[st] * dt), s->stream);
+      T *t = a;
+      a = b;
+      b = t;
+    }
+    return e;
+  }
   if (s->phys.visc > 0) {
     T *Q = (T *)s->Q, *rhs = (T *)s->rhs, *gQ = (T *)s->gradQ, *rg = (T *)s->rhs_gradQ;
     for (int st = 0; st < 5 && e == cudaSuccess; ++st) {
@@ -110,7 +141,7 @@ int capture(cb_solver *s, double dt) {
   cudaError_t e = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal);
   if (e != cudaSuccess) return solver_fail(CB_ERR_CUDA, "begin capture: %s", cudaGetErrorString(e));
   cudaError_t e1 = enqueue(s, dt, true);
-  if (s->phys.visc <= 0 && e1 == cudaSuccess) e1 = enqueue(s, dt, false);  // two steps
+  if (pingpong(s) && e1 == cudaSuccess) e1 = enqueue(s, dt, false);  // two steps
   e = cudaStreamEndCapture(s->stream, &s->graph);
   if (e1 != cudaSuccess || e != cudaSuccess) {
     drop_graph(s);
@@ -178,10 +209,13 @@ int cb_solver_create(cb_solver **out, int dim, int N, int precision, int64_t nel
   if (phys->visc > 0) {
     const size_t gbytes = w * (size_t)Np * ns * dim * nelem;
     if ((e = cudaMalloc(&s->gradQ, gbytes)) != cudaSuccess) return bail(CB_ERR_NOMEM, "gradQ");
-    if ((e = cudaMalloc(&s->rhs_gradQ, gbytes)) != cudaSuccess) return bail(CB_ERR_NOMEM, "rhs_gradQ");
     cudaMemsetAsync(s->gradQ, 0, gbytes, s->stream);
-    cudaMemsetAsync(s->rhs_gradQ, 0, gbytes, s->stream);
-  } else {
+    if (!fused_visc(s)) {
+      if ((e = cudaMalloc(&s->rhs_gradQ, gbytes)) != cudaSuccess) return bail(CB_ERR_NOMEM, "rhs_gradQ");
+      cudaMemsetAsync(s->rhs_gradQ, 0, gbytes, s->stream);
+    }
+  }
+  if (pingpong(s)) {
     if ((e = cudaMalloc(&s->Qalt, w * (size_t)Np * ns * nelem)) != cudaSuccess) return bail(CB_ERR_NOMEM, "state twin");
     if ((e = cudaMalloc(&s->nbr, sizeof(int32_t) * nface * nelem)) != cudaSuccess) return bail(CB_ERR_NOMEM, "neighbours");
   }
@@ -203,7 +237,7 @@ int cb_solver_create(cb_solver **out, int dim, int N, int precision, int64_t nel
   }
   e = precision == 64 ? ops<double>(s)->prepare() : ops<float>(s)->prepare();
   if (e != cudaSuccess) return bail(CB_ERR_CUDA, "kernel attributes");
-  if (phys->visc <= 0) {
+  if (pingpong(s)) {
     const Ops<double> *o = ops<double>(s);
     if ((e = o->build_nbr(s->nbr, vmapM, vmapP, elemtobndy, nelem, s->status, s->stream)) != cudaSuccess)
       return bail(CB_ERR_CUDA, "neighbour table");
@@ -228,7 +262,7 @@ int cb_lsrk_run(cb_solver *s, int64_t nsteps, double dt) {
   if (!s) return solver_fail(CB_ERR_ARG, "null solver");
   if (nsteps < 0) return solver_fail(CB_ERR_ARG, "nsteps must be >= 0");
   if (nsteps == 0) return CB_OK;
-  const int64_t per_graph = s->phys.visc > 0 ? 1 : 2;
+  const int64_t per_graph = pingpong(s) ? 2 : 1;
   const int64_t reps = nsteps / per_graph, rem = nsteps % per_graph;
   cudaError_t e;
   if (reps > 0) {
@@ -289,9 +323,10 @@ int cb_solver_sums(cb_solver *s, double *out_host) {
 
 int cb_solver_set_offset(cb_solver *s, const double *qref) {
   if (!s || !qref) return solver_fail(CB_ERR_ARG, "null argument");
-  if (s->phys.visc > 0) {
+  if (s->phys.visc > 0 && !fused_visc(s)) {
     for (int k = 0; k < (s->dim == 2 ? 4 : 5); ++k)
-      if (qref[k] != 0.0) return solver_fail(CB_ERR_UNSUPPORTED, "state offsets are supported by the inviscid form only");
+      if (qref[k] != 0.0)
+        return solver_fail(CB_ERR_UNSUPPORTED, "state offsets: the viscous form of this order has none");
     return CB_OK;
   }
   for (int k = 0; k < (s->dim == 2 ? 4 : 5); ++k) s->qref[k] = qref[k];

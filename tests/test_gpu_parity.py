@@ -285,6 +285,31 @@ def test_viscous_solver_vortex():
     s.close()
 
 
+@pytest.mark.parametrize("N,walls", [(3, True), (5, False), (8, True)])
+def test_viscous_solver_3d(N, walls):
+    """cb_lsrk_run with visc > 0: orders 3 and 5 run the two fused passes per
+    stage, order 8 (groups of more than two nodes per thread) the unfused
+    reference sequence; both against the oracle, and the fused form with
+    state offsets (Q stored as Q - qref) to the same tolerance."""
+    m = make_mesh(3, N, n=2, periodic=not walls)
+    ph = dict(dg.WORKLOAD_PHYS, visc=0.02)
+    Q = random_state(m, 11)
+    dt, k = 2e-4, 3
+    ref, rref = Q.copy(order="F"), np.zeros_like(Q, order="F")
+    O.lowstorageRK(3, N, m.vgeo, m.sgeo, ref, rref, m.D, dt, k, m.vmapM, m.vmapP, m.elemtobndy,
+                   oracle_phys(ph), NT)
+    s = dg.LSRK.for_state(dg.DeviceMesh.upload(m), Q, 64, phys=dg.make_phys(**ph))
+    s.run(k, dt)
+    assert relerr(s.state(), ref) < 1e-12
+    s.close()
+    if N < 8:
+        off = Q.mean(axis=(0, 2))
+        s = dg.LSRK.for_state(dg.DeviceMesh.upload(m), Q, 64, phys=dg.make_phys(**ph), offset=off)
+        s.run(k, dt)
+        assert relerr(s.state(), ref) < 1e-12
+        s.close()
+
+
 def test_invalid_boundary_code_is_reported():
     import torch
     from canary_b200._lib import CanaryError, CB_ERR_BC
