@@ -205,7 +205,7 @@ __device__ __forceinline__ void stage_group(const BDesc<T> &I, int64_t e0, int n
 // Persistent grouped stage kernel of one shape: the blocks stride over the
 // shape's work list.
 template <int DIM, int Nq, int G, typename T>
-__global__ void __launch_bounds__(BT, 2)
+__global__ void __launch_bounds__(BT, sizeof(T) == 4 ? 2 : 1)
 k_stage_batch(const BHdr *__restrict__ hdr, int stage, PhysT<T> p, T rka, double rkb) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int SID = shape_id(DIM, Nq - 1, 1 + G);
@@ -521,7 +521,7 @@ __device__ __forceinline__ void ns_stage_group(const BDesc<T> &I, const T *__res
 
 // Persistent viscous passes of one shape (the grouped variant's work list).
 template <int DIM, int Nq, typename T, bool GRAD>
-__global__ void __launch_bounds__(BT, 1)
+__global__ void __launch_bounds__(BT, sizeof(T) == 4 ? 2 : 1)
 k_ns_batch(const BHdr *__restrict__ hdr, int stage, PhysT<T> p, T rka, double rkb) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int SID = shape_id(DIM, Nq - 1, 1);
@@ -548,7 +548,7 @@ k_ns_batch(const BHdr *__restrict__ hdr, int stage, PhysT<T> p, T rka, double rk
 // of BCfg<DIM, Nq, 0>::EPB consecutive elements, blocks striding over them;
 // the state is read from I.Q[0] and written to I.Q[1].
 template <int DIM, int Nq, typename T, bool GRAD>
-__global__ void __launch_bounds__(BT, 1)
+__global__ void __launch_bounds__(BT, sizeof(T) == 4 ? 2 : 1)
 k_ns_mesh(BDesc<T> I, T *gq, int64_t nelem, PhysT<T> p, T rka, T rkbdt) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int EPB = BCfg<DIM, Nq, 0>::EPB;
