@@ -63,7 +63,8 @@ struct Pipe2 {
   static constexpr int NSB = DEEP ? 2 : 1, NTB = DEEP ? 3 : 2;  // S and T slabs
   static constexpr int LOOK = DEEP ? 2 : 1;  // groups ahead whose copies are issued
   static constexpr size_t OFF_D = DEEP ? 48 : 32;  // NSB + NTB mbarriers before
-  static constexpr size_t OFF_S = OFF_D + pad16(sizeof(T) * Nq * RS);
+  // D rows, then (AFF) the LGL weights
+  static constexpr size_t OFF_S = OFF_D + pad16(sizeof(T) * Nq * RS) + (AFF ? pad16(sizeof(T) * Nq) : 0);
   static constexpr size_t SBYTES = C::EPB * (QB + GBP);
   static constexpr size_t OFF_T = OFF_S + NSB * pad16(SBYTES);
   static constexpr size_t TBYTES = C::EPB * (QB + SB);
@@ -201,6 +202,13 @@ k_stage_pipe2(Src src, PhysT<T> p, T rka) {
     }
   };
   load_nbr(0, nbn);
+  // AFF: the LGL weights head every mesh's record array (the same for every
+  // mesh of this order)
+  const T *WS = DT + Nq * RS;
+  if constexpr (AFF) {
+    if (tid < Nq && src.valid(0)) const_cast<T *>(WS)[tid] = src.vgeo(0)[tid];
+    __syncthreads();
+  }
 
   bool timed_out = false;
   const T *curD = nullptr;  // derivative matrix held in DT (rows padded like the flux rows)
@@ -272,7 +280,7 @@ k_stage_pipe2(Src src, PhysT<T> p, T rka) {
 #pragma unroll
             for (int c = 0; c < DIM; ++c) met[r][c] = G[r + DIM * c];
           // M = kron(w, w[, w]) in computegeometry's multiplication order
-          const T M = DIM == 2 ? vgeo[j] * vgeo[i] : (vgeo[k] * vgeo[j]) * vgeo[i];
+          const T M = DIM == 2 ? WS[j] * WS[i] : (WS[k] * WS[j]) * WS[i];
           MJ = M * G[DIM * DIM];
           mji[u] = T(1) / MJ;
         } else {
@@ -312,7 +320,7 @@ k_stage_pipe2(Src src, PhysT<T> p, T rka) {
           const T *rec = Sg + el * GS + DIM * DIM + 1 + f * (DIM + 1);
 #pragma unroll
           for (int c = 0; c < DIM; ++c) nrm[c] = rec[c];
-          const T sM = DIM == 2 ? vgeo[fn] : vgeo[fn / Nq] * vgeo[fn % Nq];
+          const T sM = DIM == 2 ? WS[fn] : WS[fn / Nq] * WS[fn % Nq];
           smj = sM * rec[DIM];
         } else {
           const T *sg = Ts + (size_t)NSG * (fn + Nfp * (f + NF * el));
