@@ -63,7 +63,7 @@ __global__ void k_batch_admit(BHdr *hdr, int sid, int slot, BDesc<T> d, void *gq
   BWork *work = hdr->work[sid];
   for (int g = t; g < ngroups; g += gridDim.x * blockDim.x) {
     const int64_t e0 = (int64_t)g * epb, rem = nelem - e0;
-    work[pos + g] = BWork{slot, (int32_t)e0, rem < epb ? (int32_t)rem : epb, 1};
+    work[pos + g] = BWork{slot, (int32_t)e0, rem < epb ? (int32_t)rem : epb, rem <= epb ? 3 : 1};
   }
 }
 
@@ -581,6 +581,8 @@ int cb_mesh_create(cb_mesh **out, int dim, int N, int precision, int64_t nelem, 
   if (nelem <= 0 || nelem > (1ll << 28)) return solver_fail(CB_ERR_ARG, "cb_mesh_create: bad element count");
   if (!vgeo || !sgeo || !vmapM || !vmapP || !elemtobndy || !D)
     return solver_fail(CB_ERR_ARG, "cb_mesh_create: null array");
+  if (((uintptr_t)vgeo | (uintptr_t)sgeo) & 15)
+    return solver_fail(CB_ERR_ARG, "cb_mesh_create: vgeo and sgeo must be 16-byte aligned");
   cudaStream_t st = (cudaStream_t)stream;
   cb_mesh *m = new cb_mesh();
   m->dim = dim;
@@ -769,6 +771,8 @@ int cb_batch_add(cb_batch *b, const cb_mesh *m, void *Q, void *rhs, double dt, i
   if (!b || !m || !Q || !rhs || !slot || nsteps < 0 || !std::isfinite(dt))
     return solver_fail(CB_ERR_ARG, "cb_batch_add: bad arguments");
   if (m->prec != b->prec) return solver_fail(CB_ERR_ARG, "cb_batch_add: mesh precision differs from the batch's");
+  if (((uintptr_t)Q | (uintptr_t)rhs) & 15)
+    return solver_fail(CB_ERR_ARG, "cb_batch_add: Q and rhs must be 16-byte aligned");
   return b->prec == 64 ? batch_add<double>(b, m, Q, rhs, dt, nsteps, qref, slot)
                        : batch_add<float>(b, m, Q, rhs, dt, nsteps, qref, slot);
 }

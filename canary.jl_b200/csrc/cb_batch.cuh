@@ -43,8 +43,9 @@ struct alignas(16) BDesc {
   T qref[5];
 };
 // One work item: a group of `nv` consecutive elements (from e0) of the
-// instance in `slot`; written when the instance is admitted and invalidated
-// (valid = 0) when it is released.
+// instance in `slot`; written when the instance is admitted (valid = 1, or 3
+// for the instance's last group) and invalidated (valid = 0) when it is
+// released.
 struct alignas(16) BWork {
   int32_t slot, e0, nv, valid;
 };
@@ -581,7 +582,7 @@ template <typename T>
 struct BItem {
   BDesc<T> d;  // word-for-word copy of the instance descriptor
   int64_t e0;
-  int32_t nv, valid, par, pad;
+  int32_t nv, valid, par, last;  // last: the group ends the instance's arrays
 };
 struct alignas(16) BRingHdr {
   const BWork *work;
@@ -627,6 +628,7 @@ struct BatchSrc {
       if (lane == 0) {
         dst.e0 = wk.e0;
         dst.nv = wk.nv;
+        dst.last = wk.valid >> 1;
         dst.par = (int)((step - start + stage) & 1);
         dst.valid = 1;
       }
@@ -668,6 +670,7 @@ struct BatchSrc {
   }
   __device__ const BItem<T> &at(int it) const { return ring[it % RING]; }
   __device__ bool valid(int it) const { return at(it).valid != 0; }
+  __device__ bool last(int it) const { return at(it).last != 0; }
   __device__ int64_t e0(int it) const { return at(it).e0; }
   __device__ int nv(int it) const { return at(it).nv; }
   __device__ const T *Qin(int it) const { return at(it).d.Q[at(it).par]; }

@@ -36,6 +36,14 @@ namespace cb {
 // [w (Nq, padded to 16 bytes) | record of element 0 | record of element 1 ...]
 // (built by cb_mesh_create for meshes whose elements are all affine).
 //
+// RAG: element slabs whose byte sizes are not multiples of 16 (3-D even
+// orders, where Np is odd).  Each copy then starts at the 16-byte boundary
+// at or below its source and lands `head` bytes into its shared-memory slab,
+// and ends at the boundary at or above its end — the extra bytes belong to
+// the neighbouring elements of the same array and are not used — except for
+// a group that ends its array: there the last (< 16) bytes are loaded by the
+// issuing thread with plain loads.  Slabs carry 32 bytes of slack.
+//
 // DEEP: copies run two groups ahead instead of one — two S slabs (S of group
 // it + 2 is issued when group it releases its slab) and three T slabs (T of
 // group it + 2 is issued at the top of iteration it) — so that a block keeps
@@ -52,22 +60,26 @@ struct Pipe2 {
   static constexpr int AW = DIM * DIM + 1 + 2 * DIM * (DIM + 1);  // affine record values
   static constexpr size_t AGB = pad16(sizeof(T) * AW);             // affine record bytes
   static constexpr int WOFF = (int)(pad16(sizeof(T) * Nq) / sizeof(T));  // records after the weights
-  // the metric fields of an element are copied as one padded run (the pad
-  // reads the start of the coordinate fields, which are never used)
-  static constexpr size_t GBP = AFF ? AGB : pad16(GB);
-  static constexpr int GS = (int)(GBP / sizeof(T));  // element stride of the staged metric / record
   static constexpr size_t VB = sizeof(T) * (size_t)C::Np * NVG;  // vgeo bytes per element
   static constexpr size_t SB = AFF ? 0 : sizeof(T) * (size_t)NSG * C::Nfp * C::NFACE;  // sgeo per element
-  static constexpr bool BULK =
-      AFF ? QB % 16 == 0 : (QB % 16 == 0 && VB % 16 == 0 && SB % 16 == 0 && GBP <= VB);
+  static constexpr bool RAG = QB % 16 != 0 || VB % 16 != 0 || SB % 16 != 0;
+  static constexpr size_t SLK = RAG ? 32 : 0;
+  // the metric fields of an element are copied as one padded run (the pad
+  // reads the start of the coordinate fields, which are never used)
+  static constexpr size_t GBP = AFF ? AGB : pad16(GB) + (RAG ? 16 : 0);
+  static constexpr size_t GCOPY = RAG ? GB : GBP;  // bytes asked for per element metric copy
+  static constexpr int GS = (int)(GBP / sizeof(T));  // element stride of the staged metric / record
+  static constexpr size_t QBS = pad16(C::EPB * QB + SLK);            // staged state / carry per slab
+  static constexpr size_t SGS = AFF ? 0 : pad16(C::EPB * SB + SLK);  // staged sgeo per slab
+  static constexpr bool BULK = AFF || pad16(GB) + 16 <= VB;
   static constexpr int NSB = DEEP ? 2 : 1, NTB = DEEP ? 3 : 2;  // S and T slabs
   static constexpr int LOOK = DEEP ? 2 : 1;  // groups ahead whose copies are issued
   static constexpr size_t OFF_D = DEEP ? 48 : 32;  // NSB + NTB mbarriers before
   // D rows, then (AFF) the LGL weights
   static constexpr size_t OFF_S = OFF_D + pad16(sizeof(T) * Nq * RS) + (AFF ? pad16(sizeof(T) * Nq) : 0);
-  static constexpr size_t SBYTES = C::EPB * (QB + GBP);
+  static constexpr size_t SBYTES = QBS + C::EPB * GBP;
   static constexpr size_t OFF_T = OFF_S + NSB * pad16(SBYTES);
-  static constexpr size_t TBYTES = C::EPB * (QB + SB);
+  static constexpr size_t TBYTES = QBS + SGS;
   static constexpr size_t OFF_F = OFF_T + NTB * pad16(TBYTES);
   static constexpr size_t FDIR = P1::FDIR;
   static constexpr size_t FLUX = sizeof(T) * DIM * FDIR;
@@ -104,6 +116,7 @@ struct MeshSrc {
   __device__ void publish(int) {}
   __device__ int64_t g(int it) const { return (int64_t)blockIdx.x + (int64_t)it * gridDim.x; }
   __device__ bool valid(int it) const { return g(it) * EPB < nelem; }
+  __device__ bool last(int it) const { return (g(it) + 1) * EPB >= nelem; }  // the group ends the arrays
   __device__ int64_t e0(int it) const { return g(it) * EPB; }
   __device__ int nv(int it) const {
     const int64_t r = nelem - e0(it);
@@ -147,30 +160,66 @@ k_stage_pipe2(Src src, PhysT<T> p, T rka) {
   T *FF = reinterpret_cast<T *>(smem_raw + PP::OFF_FF);
   const int tid = threadIdx.x;
 
+  // Byte offset of a source within its 16-byte line (0 unless RAG).
+  auto head_of = [](const T *g) -> uint32_t {
+    return PP::RAG ? (uint32_t)(reinterpret_cast<uintptr_t>(g) & 15) : 0u;
+  };
+  // One slab copy of n bytes from g into the 16-byte aligned dst (see RAG):
+  // returns the bulk bytes and issues the copy when `go`; `last`: the copy
+  // ends its array, so it stops at the boundary below the end and `tail`
+  // loads the rest.
+  auto rag = [&](T *dst, const T *g, size_t n, bool last, uint64_t *bar, bool go) -> uint32_t {
+    const uint32_t head = head_of(g);
+    const uint32_t end = head + (uint32_t)n;
+    const uint32_t L = PP::RAG ? (last ? (end & ~15u) : ((end + 15u) & ~15u)) : end;
+    if (go && L) bulk_g2s(dst, reinterpret_cast<const unsigned char *>(g) - head, L, bar);
+    return L;
+  };
+  auto tail = [&](T *dst, const T *g, size_t n) {
+    const uint32_t head = head_of(g);
+    const uint32_t end = head + (uint32_t)n;
+    const unsigned char *base = reinterpret_cast<const unsigned char *>(g) - head;
+    for (uint32_t b = (end & ~15u) > head ? (end & ~15u) : head; b < end; b += sizeof(T))
+      *reinterpret_cast<T *>(reinterpret_cast<unsigned char *>(dst) + b) = *reinterpret_cast<const T *>(base + b);
+  };
   auto issue_S = [&](int it, int b) {  // thread 0 only
     const int64_t e0 = src.e0(it);
     const int nv = src.nv(it);
-    const T *q = src.Qin(it), *vg = src.vgeo(it);
-    T *dq = S0 + b * SSTRIDE, *dg = dq + EPB * Np * NS;
+    const bool last = PP::RAG && src.last(it);
+    const T *q = src.Qin(it) + e0 * Np * NS, *vg = src.vgeo(it);
+    T *dq = S0 + b * SSTRIDE, *dg = dq + PP::QBS / sizeof(T);
+    uint32_t tx = rag(dq, q, nv * PP::QB, last, &barS[b], false);
+    if constexpr (AFF) {
+      tx += (uint32_t)(nv * PP::GBP);
+    } else {
+      for (int el = 0; el < nv; ++el) tx += rag(dg + el * GS, vg + (e0 + el) * Np * NVG, PP::GCOPY, false, &barS[b], false);
+    }
+    if (last) tail(dq, q, nv * PP::QB);
     fence_proxy_async();
-    mbar_expect_tx(&barS[b], (uint32_t)(nv * (PP::QB + PP::GBP)));
-    bulk_g2s(dq, q + e0 * Np * NS, (uint32_t)(nv * PP::QB), &barS[b]);
+    mbar_expect_tx(&barS[b], tx);
+    rag(dq, q, nv * PP::QB, last, &barS[b], true);
     if constexpr (AFF) {  // the group's records are contiguous
       bulk_g2s(dg, vg + PP::WOFF + e0 * GS, (uint32_t)(nv * PP::GBP), &barS[b]);
     } else {
-      for (int el = 0; el < nv; ++el)
-        bulk_g2s(dg + el * GS, vg + (e0 + el) * Np * NVG, (uint32_t)PP::GBP, &barS[b]);
+      for (int el = 0; el < nv; ++el) rag(dg + el * GS, vg + (e0 + el) * Np * NVG, PP::GCOPY, false, &barS[b], true);
     }
   };
   auto issue_T = [&](int it, int b) {  // thread 0 only
     const int64_t e0 = src.e0(it);
     const int nv = src.nv(it);
-    T *dc = T0 + b * TSTRIDE, *ds = dc + EPB * Np * NS;
+    const bool last = PP::RAG && src.last(it);
+    const T *c = src.rhs(it) + e0 * Np * NS, *sg = src.sgeo(it) + e0 * (int64_t)(PP::SB / sizeof(T));
+    T *dc = T0 + b * TSTRIDE, *ds = dc + PP::QBS / sizeof(T);
+    uint32_t tx = rag(dc, c, nv * PP::QB, last, &barT[b], false);
+    if constexpr (!AFF) tx += rag(ds, sg, nv * PP::SB, last, &barT[b], false);
+    if (last) {
+      tail(dc, c, nv * PP::QB);
+      if constexpr (!AFF) tail(ds, sg, nv * PP::SB);
+    }
     fence_proxy_async();
-    mbar_expect_tx(&barT[b], (uint32_t)(nv * (PP::QB + PP::SB)));
-    bulk_g2s(dc, src.rhs(it) + e0 * Np * NS, (uint32_t)(nv * PP::QB), &barT[b]);
-    if constexpr (!AFF)
-      bulk_g2s(ds, src.sgeo(it) + e0 * (PP::SB / sizeof(T)), (uint32_t)(nv * PP::SB), &barT[b]);
+    mbar_expect_tx(&barT[b], tx);
+    rag(dc, c, nv * PP::QB, last, &barT[b], true);
+    if constexpr (!AFF) rag(ds, sg, nv * PP::SB, last, &barT[b], true);
   };
 
   src.begin(smem_raw + PP::smem());
@@ -245,8 +294,12 @@ k_stage_pipe2(Src src, PhysT<T> p, T rka) {
     // ---- wait for S[sb] (state + metric) and T[tb] (carry + sgeo)
     if (!mbar_wait_bounded(&barS[sb], (uint32_t)((it / PP::NSB) & 1), WAIT_LIMIT)) timed_out = true;
     if (!mbar_wait_bounded(&barT[tb], (uint32_t)((it / PP::NTB) & 1), WAIT_LIMIT)) timed_out = true;
-    const T *Sq = S0 + sb * SSTRIDE, *Sg = Sq + EPB * Np * NS;
-    const T *Tc = T0 + tb * TSTRIDE, *Ts = Tc + EPB * Np * NS;
+    // staged slabs (RAG: each source's data starts `head` bytes into its slab)
+    const T *Sq = S0 + sb * SSTRIDE + head_of(Qin + e0 * Np * NS) / sizeof(T);
+    const T *Sg = S0 + sb * SSTRIDE + PP::QBS / sizeof(T);
+    const T *Tc = T0 + tb * TSTRIDE + head_of(src.rhs(it) + e0 * Np * NS) / sizeof(T);
+    const T *Ts = T0 + tb * TSTRIDE + PP::QBS / sizeof(T) +
+                  (AFF ? 0 : head_of(src.sgeo(it) + e0 * (int64_t)(PP::SB / sizeof(T))) / sizeof(T));
     const T *__restrict__ vgeo = src.vgeo(it);
     if (src.D(it) != curD) {  // read in phase B only; visible after the mid barrier
       curD = src.D(it);
@@ -271,7 +324,7 @@ k_stage_pipe2(Src src, PhysT<T> p, T rka) {
           qd[u][s] = Sq[(el * NS + s) * Np + n];
           q[s] = qd[u][s] + qr[s];
         }
-        const T *G = Sg + el * GS;
+        const T *G = Sg + el * GS + (AFF ? 0 : head_of(vgeo + (e0 + el) * Np * NVG) / sizeof(T));
         const int i = n % Nq, j = (n / Nq) % Nq, k = DIM == 3 ? n / (Nq * Nq) : 0;
         T met[DIM][DIM], MJ, gc = T(0);
         if constexpr (AFF) {

@@ -268,7 +268,8 @@ int cb_batch_set_affine(cb_batch *b, int on);
  * during the following cb_batch_run calls.  qref (nstate doubles, or NULL for
  * zeros) are per-field offsets as in cb_solver_set_offset (Q holds Q - qref).
  * Writes the slot id.  The batch keeps a twin state buffer from its own
- * stream-ordered pool. */
+ * stream-ordered pool.  Q and rhs (and the mesh's vgeo and sgeo) must be
+ * 16-byte aligned: the stage copies element slabs with bulk copies. */
 int cb_batch_add(cb_batch *b, const cb_mesh *m, void *Q, void *rhs, double dt,
                  int64_t nsteps, const double *qref, int *slot);
 /* Advance every admitted instance by nsteps steps, each stopping at its own
