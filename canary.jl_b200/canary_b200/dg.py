@@ -252,12 +252,17 @@ def build_mesh(dim, N, x, periodic, boundary=None, meshwarp=None) -> Mesh:
 
 
 def to_device(a: np.ndarray, dtype=None, device="cuda"):
-    """Column-major numpy array -> flat CUDA tensor with the same memory order."""
+    """Column-major numpy array -> flat CUDA tensor with the same memory order.
+    The copy goes through pinned memory and is ordered on the current stream
+    without waiting for it (a copy from pageable memory would first wait for
+    all earlier work of the stream)."""
     torch = _torch()
     flat = np.asarray(a).ravel(order="F")
     t = torch.from_numpy(np.ascontiguousarray(flat))
     if dtype is not None:
         t = t.to(dtype)
+    if torch.device(device).type == "cuda":
+        return t.pin_memory().to(device, non_blocking=True)
     return t.to(device)
 
 

@@ -162,14 +162,15 @@ def fourier_state_t(x, y, z, seed=0, kmax=4, gamma=GAMMA):
     """Torch form of fourier_state for device tensors x, y, z (FP64), summing
     16 wave vectors per batch; returns (U, V, W, ρ, E) tensors."""
     import torch
-    key = (seed, kmax, str(x.device))
+    from .dg import to_device
+    key = (kmax, str(x.device))
+    ks, coef = fourier_coefficients(seed, kmax)
     if key not in _FOURIER:
-        ks, coef = fourier_coefficients(seed, kmax)
-        K = torch.as_tensor(ks, dtype=torch.float64, device=x.device)
-        C = [(torch.as_tensor(a, dtype=torch.float64, device=x.device),
-              torch.as_tensor(phi, dtype=torch.float64, device=x.device)) for a, phi in coef]
-        _FOURIER[key] = (K, C)
-    K, C = _FOURIER[key]
+        _FOURIER[key] = to_device(ks, torch.float64, x.device).reshape(ks.shape[1], ks.shape[0]).t()
+    K = _FOURIER[key]
+    # the amplitudes and phases of the four fields in one upload
+    cf = to_device(np.array([v for pair in coef for v in pair]).T, torch.float64, x.device).reshape(8, -1)
+    C = [(cf[2 * q], cf[2 * q + 1]) for q in range(4)]
     X = [c.reshape(-1) for c in (x, y, z)]
     out = []
     for A, PH in C:
@@ -190,6 +191,8 @@ def device_state(fields, dtype=None, offset=None):
     nelem) column-major state, minus the per-field `offset`, cast to dtype."""
     import torch
     Q = torch.stack(fields, dim=1)  # (nelem, nstate, Np) C order == (Np, nstate, nelem) F order
-    if offset is not None:
-        Q = Q - torch.as_tensor(offset, dtype=Q.dtype, device=Q.device).view(1, -1, 1)
+    if offset is not None:  # per-field scalars (no host-to-device copy)
+        for s, o in enumerate(offset):
+            if o != 0.0:
+                Q[:, s] -= float(o)
     return Q.to(dtype or Q.dtype).contiguous().reshape(-1)

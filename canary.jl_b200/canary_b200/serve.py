@@ -163,6 +163,21 @@ class _Lane:
 
 
 @dataclass
+class _Prep:
+    """A request whose mesh and initial state are being set up on the setup
+    stream; `speed` (pinned) receives its max wave speed, `event` marks the
+    end of the set-up."""
+    req: Request
+    mesh: _Mesh
+    bytes: int
+    offset: np.ndarray
+    Q: object
+    rhs: object
+    speed: object
+    event: object
+
+
+@dataclass
 class _Live:
     req: Request
     mesh: _Mesh
@@ -227,7 +242,8 @@ class Server:
     state offsets); tick_steps steps are launched per loop iteration, with at
     most two ticks in flight."""
 
-    def __init__(self, precision=32, hbm_budget=120e9, max_instances=4096, tick_steps=8, device="cuda"):
+    def __init__(self, precision=32, hbm_budget=120e9, max_instances=4096, tick_steps=8, device="cuda",
+                 admit_slice=0.02):
         torch = _torch()
         self.torch = torch
         self.device = torch.device(device)
@@ -235,7 +251,12 @@ class Server:
         self.real = torch.float32 if precision == 32 else torch.float64
         self.budget = int(hbm_budget)
         self.tick = tick_steps
-        self.sstream = torch.cuda.Stream(self.device)  # meshes and initial states
+        # host seconds of admissions (mesh set-up, initial states) between two
+        # ticks while requests are resident, so that device work overlaps them
+        self.admit_slice = admit_slice
+        # meshes and initial states; high priority, so that set-up kernels get
+        # SMs between the batches' persistent stage kernels
+        self.sstream = torch.cuda.Stream(self.device, priority=-1)
         self.max_instances = max_instances
         # the inviscid and the viscous batch, each on its own stream (with
         # their admissions and retirements)
@@ -257,35 +278,43 @@ class Server:
             return w * n * (3 + req.dim)
         return 3 * w * n  # Q, rhs, batch-owned twin
 
-    def _initial(self, req: Request, m: _Mesh):
-        torch = self.torch
-        x = m.dmesh.coords()
-        if req.kind == "vortex":
-            f = ic.isentropic_vortex_t(x[0], x[1], req.beta, req.xc, req.yc)
-            off = np.array([1.0, 0.0, 1.0, 1.0 / (GAMMA - 1.0) + 0.5])
-        else:
-            f = ic.fourier_state_t(x[0], x[1], x[2], seed=req.seed)
-            off = np.array([0.0, 0.0, 0.0, 1.0, 1.0 / (GAMMA - 1.0)])
-        speed = float(wave_speed(f, req.dim).item())  # synchronises the setup stream only
-        if self.precision == 64:
-            off = np.zeros(nstate(req.dim))
-        Q = ic.device_state(list(f), self.real, off)
-        return Q, torch.zeros_like(Q), off, speed
-
-    def admit(self, req: Request, now: float) -> _Live:
+    def prepare(self, req: Request) -> _Prep:
+        """Reserve the request's memory and enqueue its mesh (if not cached)
+        and initial state on the setup stream, without waiting for them."""
         torch = self.torch
         m = self.pool.get(req, self.precision)
         with torch.cuda.stream(self.sstream):
-            Q, rhs, off, speed = self._initial(req, m)
-        nsteps, dt = plan(req, speed)
+            x = m.dmesh.coords()
+            if req.kind == "vortex":
+                f = ic.isentropic_vortex_t(x[0], x[1], req.beta, req.xc, req.yc)
+                off = np.array([1.0, 0.0, 1.0, 1.0 / (GAMMA - 1.0) + 0.5])
+            else:
+                f = ic.fourier_state_t(x[0], x[1], x[2], seed=req.seed)
+                off = np.array([0.0, 0.0, 0.0, 1.0, 1.0 / (GAMMA - 1.0)])
+            speed = torch.empty(1, dtype=torch.float64, pin_memory=True)
+            speed.copy_(wave_speed(f, req.dim).reshape(1), non_blocking=True)
+            if self.precision == 64:
+                off = np.zeros(nstate(req.dim))
+            Q = ic.device_state(list(f), self.real, off)
+            rhs = torch.zeros_like(Q)
+        ev = torch.cuda.Event()
+        ev.record(self.sstream)
+        nb = self.request_bytes(req)
+        self.in_use += nb
+        return _Prep(req, m, nb, off, Q, rhs, speed, ev)
+
+    def admit(self, pr: _Prep, now: float) -> _Live:
+        """Admit a prepared request (its set-up event has completed) into its
+        batch."""
+        req, Q, rhs = pr.req, pr.Q, pr.rhs
+        nsteps, dt = plan(req, float(pr.speed[0]))
         lane = self.lanes[req.kind == "ns3d"]
-        live = _Live(req, m, nsteps, dt, self.request_bytes(req), off, lane, Q, rhs, left=nsteps, admitted=now)
+        live = _Live(req, pr.mesh, nsteps, dt, pr.bytes, pr.offset, lane, Q, rhs, left=nsteps, admitted=now)
         lane.stream.wait_stream(self.sstream)
         Q.record_stream(lane.stream)
         rhs.record_stream(lane.stream)
-        live.slot = lane.batch.add(m.batch[self.precision], Q, rhs, dt, nsteps, off)
+        live.slot = lane.batch.add(pr.mesh.batch[self.precision], Q, rhs, dt, nsteps, pr.offset)
         lane.live += 1
-        self.in_use += live.bytes
         return live
 
     def _fits(self, req: Request) -> bool:
@@ -300,7 +329,7 @@ class Server:
         arrival order (a closed-loop capacity run; latencies count from 0)."""
         torch = self.torch
         reqs = deque(sorted(requests, key=lambda r: (r.arrival, r.rid)))
-        waiting, live, retiring = deque(), {}, []
+        waiting, preparing, live, retiring = deque(), deque(), {}, []
         lat, results, failed = {}, {}, set()
         flight = {}  # stream -> events of the ticks in flight
         ticks = 0
@@ -318,16 +347,25 @@ class Server:
             if len(q) > 2:  # at most two ticks in flight per stream
                 q.popleft().synchronize()
 
-        while reqs or waiting or live or retiring:
+        while reqs or waiting or preparing or live or retiring:
             now = time.perf_counter() - t0
             while reqs and (not realtime or reqs[0].arrival <= now):
                 waiting.append(reqs.popleft())
+            # set-up of arriving requests (asynchronous), then admission of
+            # those whose set-up has completed, in arrival order
+            t_adm = time.perf_counter()
             while waiting and self._fits(waiting[0]):
-                r = waiting.popleft()
-                lv = self.admit(r, time.perf_counter() - t0)
+                preparing.append(self.prepare(waiting.popleft()))
+                if time.perf_counter() - t_adm > self.admit_slice:
+                    break
+            if preparing and not live:
+                preparing[0].event.synchronize()
+            while preparing and preparing[0].event.query():
+                pr = preparing.popleft()
+                lv = self.admit(pr, time.perf_counter() - t0)
                 lv.tick0 = ticks
-                live[r.rid] = lv
-            if waiting and not live and not retiring and not self._fits(waiting[0]):
+                live[pr.req.rid] = lv
+            if waiting and not live and not retiring and not preparing and not self._fits(waiting[0]):
                 raise RuntimeError(f"request {waiting[0].rid} does not fit the HBM budget on its own")
             peak = max(peak, self.in_use + self.pool.resident_bytes())
             max_live = max(max_live, len(live))

@@ -121,10 +121,12 @@ constexpr double AFFINE_TOL = 1e-10;
 // values.  An element whose metric, J = MJ / M, normals or sJ = sMJ / sM
 // differ at any node from node 0's by more than `tol` (relative to the
 // element's largest metric term, to J, to 1 for the normals, to sJ) sets
-// *flag: the mesh is then not affine and the records are not used.
+// *flag: the mesh is then not affine and the records are not used.  Block 0
+// also writes the weights (rounded to T) to wout.
 template <typename T>
-__global__ void k_affine(int dim, int Nq, int64_t nelem, const double *vgeo, const double *sgeo, WTab wt, T *out,
-                         int gs, double tol, unsigned *flag) {
+__global__ void k_affine(int dim, int Nq, int64_t nelem, const double *vgeo, const double *sgeo, WTab wt, T *wout,
+                         T *out, int gs, double tol, unsigned *flag) {
+  if (blockIdx.x == 0 && threadIdx.x < Nq) wout[threadIdx.x] = T(wt.w[threadIdx.x]);
   const int Np = dim == 2 ? Nq * Nq : Nq * Nq * Nq, Nfp = dim == 2 ? Nq : Nq * Nq, nf = 2 * dim;
   const int nvg = dim == 2 ? 8 : 14, nsg = dim == 2 ? 4 : 5, nm = dim * dim;
   const double *w = wt.w;
@@ -243,8 +245,14 @@ struct cb_mesh {
   void *owned = nullptr;  // FP32 copies of vgeo | sgeo | D (precision 32)
   int32_t *nbr = nullptr;
   // affine-element geometry: [LGL weights | one record per element], in the
-  // mesh's precision; null when some element is not affine
+  // mesh's precision; used when every element is affine
   void *aff = nullptr;
+  // set-up status (vmap validation, affine test): device words, their pinned
+  // host copy and the event that ends the set-up; read at the first use
+  unsigned *dstat = nullptr, *hstat = nullptr;
+  cudaEvent_t ready = nullptr;
+  mutable int state = -1;  // -1: not read yet, else CB_OK, CB_ERR_BC or CB_ERR_MESH
+  mutable bool affine = false;
 };
 
 namespace {
@@ -452,6 +460,10 @@ int batch_run(cb_batch *b, int64_t nsteps) {
     }
   const int64_t launch = std::min(need, nsteps);
   if (launch <= 0) return CB_OK;
+  // keep the shapes of the current graph: a shape whose instances have all
+  // left costs a few empty launches per step, while re-building the graph
+  // each time a shape comes and goes (continuous batching) costs milliseconds
+  shapes |= b->g_shapes;
   if (!b->exec || shapes != b->g_shapes) {
     drop_graph(b);
     cudaError_t e = build_graph<T>(b, shapes);
@@ -483,7 +495,7 @@ int batch_add(cb_batch *b, const cb_mesh *m, void *Q, void *rhs, double dt, int6
   const int var = b->visc ? VAR_VISC : b->var[m->dim - 2][m->N];
   int sid = shape_id(m->dim, m->N, var);
   const BKernels<T> &K = b_kernels<T>();
-  const bool aff = !b->visc && b->affine && m->aff && b->phys.gravity == 0.0 && K.pipelined[sid] &&
+  const bool aff = !b->visc && b->affine && m->affine && b->phys.gravity == 0.0 && K.pipelined[sid] &&
                    K.fn[shape_id(m->dim, m->N, VAR_AFFINE)];
   if (aff) sid = shape_id(m->dim, m->N, VAR_AFFINE);
   const int epb = K.epb[sid];
@@ -566,6 +578,23 @@ int batch_release(cb_batch *b, int slot) {
 
 }  // namespace
 
+namespace {
+// Wait for the mesh's set-up (once) and report its validation.
+int mesh_check(const cb_mesh *m) {
+  if (m->state < 0) {
+    const cudaError_t e = cudaEventSynchronize(m->ready);
+    if (e != cudaSuccess) return solver_fail(CB_ERR_CUDA, "mesh set-up: %s", cudaGetErrorString(e));
+    const unsigned h = m->hstat[0];
+    m->affine = m->hstat[1] == 0;
+    m->state = (h & ST_BC) ? CB_ERR_BC : (h & ST_MESH) ? CB_ERR_MESH : CB_OK;
+  }
+  if (m->state == CB_ERR_BC) return solver_fail(CB_ERR_BC, "cb_mesh: invalid boundary condition code");
+  if (m->state == CB_ERR_MESH) return solver_fail(CB_ERR_MESH, "cb_mesh: vmaps do not describe a conforming mesh");
+  return CB_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 int cb_mesh_create(cb_mesh **out, int dim, int N, int precision, int64_t nelem, const double *vgeo,
@@ -591,14 +620,15 @@ int cb_mesh_create(cb_mesh **out, int dim, int N, int precision, int64_t nelem, 
   m->nelem = nelem;
   const int Nq = N + 1, nvg = dim == 2 ? 8 : 14, nsg = dim == 2 ? 4 : 5;
   const int64_t Np = dim == 2 ? (int64_t)Nq * Nq : (int64_t)Nq * Nq * Nq, Nfp = dim == 2 ? Nq : (int64_t)Nq * Nq;
-  unsigned *status = nullptr;
   cudaError_t e = cudaMalloc((void **)&m->nbr, sizeof(int32_t) * 2 * dim * nelem);
-  if (e == cudaSuccess) e = cudaMalloc((void **)&status, 2 * sizeof(unsigned));
+  if (e == cudaSuccess) e = cudaMalloc((void **)&m->dstat, 2 * sizeof(unsigned));
+  if (e == cudaSuccess) e = cudaMallocHost((void **)&m->hstat, 2 * sizeof(unsigned));
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&m->ready, cudaEventDisableTiming);
   if (e != cudaSuccess) {
     cb_mesh_destroy(m);
-    cudaFree(status);
     return solver_fail(CB_ERR_NOMEM, "cb_mesh_create: %s", cudaGetErrorString(e));
   }
+  unsigned *status = m->dstat;
   cudaMemsetAsync(status, 0, 2 * sizeof(unsigned), st);
   const Ops<double> *o = dim == 2 ? get_ops<2, double>(N) : get_ops<3, double>(N);
   e = o->build_nbr(m->nbr, vmapM, vmapP, elemtobndy, nelem, status, st);
@@ -628,41 +658,22 @@ int cb_mesh_create(cb_mesh **out, int dim, int N, int precision, int64_t nelem, 
   if (e == cudaSuccess) e = cudaMalloc(&m->aff, wsz * (woff + gs * nelem));
   if (e == cudaSuccess) {
     WTab wt{};
-    float wf[16] = {};
-    for (int i = 0; i < Nq; ++i) {
-      wt.w[i] = wl[i];
-      wf[i] = (float)wl[i];
-    }
-    e = cudaMemcpyAsync(m->aff, precision == 64 ? (const void *)wt.w : (const void *)wf, wsz * Nq,
-                        cudaMemcpyHostToDevice, st);
+    for (int i = 0; i < Nq; ++i) wt.w[i] = wl[i];
     const int blocks = (int)std::min<int64_t>(nelem, 4096);
-    if (e == cudaSuccess) {
-      if (precision == 64)
-        k_affine<double><<<blocks, 128, 0, st>>>(dim, Nq, nelem, vgeo, sgeo, wt, (double *)m->aff + woff, (int)gs,
-                                                 AFFINE_TOL, status + 1);
-      else
-        k_affine<float><<<blocks, 128, 0, st>>>(dim, Nq, nelem, vgeo, sgeo, wt, (float *)m->aff + woff, (int)gs,
-                                                AFFINE_TOL, status + 1);
-      e = cudaGetLastError();
-    }
+    if (precision == 64)
+      k_affine<double><<<blocks, 128, 0, st>>>(dim, Nq, nelem, vgeo, sgeo, wt, (double *)m->aff,
+                                               (double *)m->aff + woff, (int)gs, AFFINE_TOL, status + 1);
+    else
+      k_affine<float><<<blocks, 128, 0, st>>>(dim, Nq, nelem, vgeo, sgeo, wt, (float *)m->aff,
+                                              (float *)m->aff + woff, (int)gs, AFFINE_TOL, status + 1);
+    e = cudaGetLastError();
   }
-  unsigned h = 0, ha = 0;
-  if (e == cudaSuccess && (e = cudaMemcpyAsync(&h, status, sizeof h, cudaMemcpyDeviceToHost, st)) == cudaSuccess &&
-      (e = cudaMemcpyAsync(&ha, status + 1, sizeof ha, cudaMemcpyDeviceToHost, st)) == cudaSuccess)
-    e = cudaStreamSynchronize(st);
-  cudaFree(status);
-  if (e == cudaSuccess && ha) {
-    cudaFree(m->aff);
-    m->aff = nullptr;
-  }
+  // the status words are read at the first use of the mesh (no wait here)
+  if (e == cudaSuccess) e = cudaMemcpyAsync(m->hstat, status, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaEventRecord(m->ready, st);
   if (e != cudaSuccess) {
     cb_mesh_destroy(m);
     return solver_fail(CB_ERR_CUDA, "cb_mesh_create: %s", cudaGetErrorString(e));
-  }
-  if (h & (ST_BC | ST_MESH)) {
-    cb_mesh_destroy(m);
-    return (h & ST_BC) ? solver_fail(CB_ERR_BC, "cb_mesh_create: invalid boundary condition code")
-                       : solver_fail(CB_ERR_MESH, "cb_mesh_create: vmaps do not describe a conforming mesh");
   }
   *out = m;
   return CB_OK;
@@ -670,15 +681,21 @@ int cb_mesh_create(cb_mesh **out, int dim, int N, int precision, int64_t nelem, 
 
 int cb_mesh_affine(const cb_mesh *m, int *affine) {
   if (!m || !affine) return solver_fail(CB_ERR_ARG, "cb_mesh_affine: null argument");
-  *affine = m->aff != nullptr;
+  const int rc = mesh_check(m);
+  if (rc) return rc;
+  *affine = m->affine ? 1 : 0;
   return CB_OK;
 }
 
 int cb_mesh_destroy(cb_mesh *m) {
   if (!m) return CB_OK;
+  if (m->ready) cudaEventSynchronize(m->ready);
   cudaFree(m->nbr);
   cudaFree(m->owned);
   cudaFree(m->aff);
+  cudaFree(m->dstat);
+  if (m->hstat) cudaFreeHost(m->hstat);
+  if (m->ready) cudaEventDestroy(m->ready);
   delete m;
   return CB_OK;
 }
@@ -773,6 +790,7 @@ int cb_batch_add(cb_batch *b, const cb_mesh *m, void *Q, void *rhs, double dt, i
   if (m->prec != b->prec) return solver_fail(CB_ERR_ARG, "cb_batch_add: mesh precision differs from the batch's");
   if (((uintptr_t)Q | (uintptr_t)rhs) & 15)
     return solver_fail(CB_ERR_ARG, "cb_batch_add: Q and rhs must be 16-byte aligned");
+  if (const int rc = mesh_check(m)) return rc;
   return b->prec == 64 ? batch_add<double>(b, m, Q, rhs, dt, nsteps, qref, slot)
                        : batch_add<float>(b, m, Q, rhs, dt, nsteps, qref, slot);
 }

@@ -221,8 +221,10 @@ int cb_computegeometry(int dim, int N, int64_t nelem, const double *elemtocoord,
  *
  * A cb_mesh holds what instances on the same mesh share: the geometry (the
  * caller's FP64 arrays for precision 64, rounded FP32 copies for precision 32)
- * and the int32 face-neighbour table built from vmapM/vmapP/elemtobndy.  It
- * validates the vmaps (CB_ERR_MESH, CB_ERR_BC) and synchronises `stream`.  A
+ * and the int32 face-neighbour table built from vmapM/vmapP/elemtobndy.  Its
+ * set-up is enqueued on `stream` without waiting for it; the validation of
+ * the vmaps (CB_ERR_MESH, CB_ERR_BC) is reported by the first cb_mesh_affine
+ * or cb_batch_add that uses the mesh, which waits for the set-up once.  A
  * mesh must outlive the batch instances that use it. */
 typedef struct cb_mesh cb_mesh;
 int cb_mesh_create(cb_mesh **out, int dim, int N, int precision,

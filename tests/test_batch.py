@@ -215,3 +215,20 @@ def test_autotuner_picks_a_built_variant():
         assert b.variant(dim, N) == v
     b.close()
     assert (3, 4) in tuned and tuned[(3, 4)] in B.VARIANTS
+
+
+def test_invalid_mesh_is_reported_at_first_use(cases):
+    """cb_mesh_create does not wait for its set-up; the vmap / boundary-code
+    validation is reported by the first use of the mesh."""
+    m, Q, dt, k = cases[0]
+    dm = dg.DeviceMesh.upload(m)
+    dm.elemtobndy[0] = 7  # no such boundary condition
+    bm = B.BatchMesh(dm, 64)
+    with pytest.raises(CanaryError) as ei:
+        bm.affine
+    assert "boundary" in str(ei.value)
+    b = B.Batch(64, 2)
+    with pytest.raises(CanaryError):
+        b.add_state(bm, Q, dt, k)
+    b.close()
+    bm.close()
