@@ -548,14 +548,35 @@ k_ns_batch(const BHdr *__restrict__ hdr, int stage, PhysT<T> p, T rka, double rk
 // The two viscous passes over one mesh (cb_lsrk_run with visc > 0): groups
 // of BCfg<DIM, Nq, 0>::EPB consecutive elements, blocks striding over them;
 // the state is read from I.Q[0] and written to I.Q[1].
+// Block-wide L2 prefetch of `bytes` bytes from p (one request per 128-byte line).
+__device__ __forceinline__ void prefetch_l2(const void *p, size_t bytes) {
+  const char *c = static_cast<const char *>(p);
+  for (size_t off = (size_t)threadIdx.x * 128; off < bytes; off += (size_t)blockDim.x * 128)
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(c + off));
+}
+
 template <int DIM, int Nq, typename T, bool GRAD>
 __global__ void __launch_bounds__(BT, sizeof(T) == 4 ? 2 : 1)
 k_ns_mesh(BDesc<T> I, T *gq, int64_t nelem, PhysT<T> p, T rka, T rkbdt) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  constexpr int EPB = BCfg<DIM, Nq, 0>::EPB;
+  using C = BCfg<DIM, Nq, 0>;
+  constexpr int EPB = C::EPB, NS = Lay<DIM>::NS, NVG = Lay<DIM>::NVG, NSG = Lay<DIM>::NSG;
+  constexpr size_t QE = (size_t)C::Np * NS, VE = (size_t)C::Np * NVG, SE = (size_t)NSG * C::Nfp * C::NFACE;
   for (int64_t g = blockIdx.x; g * EPB < nelem; g += gridDim.x) {
     const int64_t e0 = g * EPB;
     const int nv = nelem - e0 < EPB ? (int)(nelem - e0) : EPB;
+    // the block's next group: bring its slabs into L2 while this one runs
+    const int64_t n0 = e0 + (int64_t)gridDim.x * EPB;
+    if (n0 < nelem) {
+      const size_t nn = (size_t)(nelem - n0 < EPB ? nelem - n0 : EPB);
+      prefetch_l2(I.Q[0] + n0 * QE, sizeof(T) * nn * QE);
+      prefetch_l2(I.vgeo + n0 * VE, sizeof(T) * nn * VE);
+      prefetch_l2(I.sgeo + n0 * SE, sizeof(T) * nn * SE);
+      if constexpr (!GRAD) {
+        prefetch_l2(I.rhs + n0 * QE, sizeof(T) * nn * QE);
+        prefetch_l2(gq + n0 * QE * DIM, sizeof(T) * nn * QE * DIM);
+      }
+    }
     if constexpr (GRAD)
       ns_grad_group<DIM, Nq, T>(I, gq, e0, nv, 0, p, smem_raw);
     else
