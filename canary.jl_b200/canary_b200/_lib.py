@@ -25,7 +25,7 @@ EXPORTS = (
     "cb_volume_grad", "cb_flux_grad", "cb_update_gradQ", "cb_volume_div", "cb_flux_div",
     "cb_solver_create", "cb_lsrk_run", "cb_solver_set_offset", "cb_solver_sums",
     "cb_solver_destroy", "cb_solver_status_async", "cb_lsrk_stage_noalloc",
-    "cb_computegeometry", "cb_mesh_create", "cb_mesh_affine", "cb_mesh_destroy",
+    "cb_computegeometry", "cb_brickmesh", "cb_mesh_create", "cb_mesh_affine", "cb_mesh_destroy",
     "cb_batch_create", "cb_batch_set_variant", "cb_batch_get_variant", "cb_batch_set_affine",
     "cb_batch_slot_variant", "cb_batch_add",
     "cb_batch_run", "cb_batch_info", "cb_batch_release", "cb_batch_status", "cb_batch_status_async", "cb_batch_destroy",
@@ -86,6 +86,7 @@ def lib() -> C.CDLL:
     L.cb_computegeometry.argtypes = [C.c_int, C.c_int, i64, vp, dbl, vp, vp, vp, vp, vp, vp]
     L.cb_mesh_create.argtypes = [C.POINTER(vp), C.c_int, C.c_int, C.c_int, i64, vp, vp, vp, vp, vp, vp, vp]
     L.cb_mesh_destroy.argtypes = [vp]
+    L.cb_brickmesh.argtypes = [C.c_int, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp, vp]
     L.cb_mesh_affine.argtypes = [vp, C.POINTER(C.c_int)]
     L.cb_batch_set_affine.argtypes = [vp, C.c_int]
     L.cb_batch_slot_variant.argtypes = [vp, C.c_int, C.POINTER(C.c_int)]

@@ -287,35 +287,63 @@ class DeviceMesh:
     D: object
 
     @classmethod
-    def build(cls, dim, N, x, periodic, warp_amp=0.0, device="cuda", boundary=None, stream=None):
-        """Connectivity on the host (brickmesh -> partition -> connectmesh ->
-        mappings, euler3d_set3c.jl:1689-1708) and the grid and geometry on the
-        device in FP64 (cb_computegeometry), with the optional warp
-        x_c += warp_amp * prod_d sin(x_d).  The returned mesh has no host
-        copies of vgeo / sgeo (mesh.vgeo / mesh.sgeo are None)."""
+    def build(cls, dim, N, x, periodic, warp_amp=0.0, device="cuda", boundary=None, stream=None,
+              connect="device"):
+        """Brick mesh, connectivity (brickmesh -> partition -> connectmesh ->
+        mappings, euler3d_set3c.jl:1689-1708) and geometry in FP64, with the
+        optional warp x_c += warp_amp * prod_d sin(x_d).  The connectivity is
+        built on the device (cb_brickmesh) or, with connect="host", by the
+        host mirror; the grid and geometry on the device (cb_computegeometry).
+        The returned mesh keeps no host copies of vgeo / sgeo (and, with the
+        device connectivity, none of the maps)."""
         torch = _torch()
         from .operators import lglpoints, spectralderivative
-        cm = connectmesh(*partition(*brickmesh(x, periodic, boundary=boundary)))
-        vmapM, vmapP = mappings(N, cm["elemtoelem"], cm["elemtoface"], cm["elemtoordr"])
         r, w = lglpoints(N)
         D = spectralderivative(r)
-        e2c = np.asarray(cm["elemtocoord"], dtype=np.float64)
-        nelem = e2c.shape[2]
         Nq = N + 1
         Np, Nfp = Nq ** dim, Nq ** (dim - 1)
         nvg, nsg = (14, 5) if dim == 3 else (8, 4)
         dev = lambda a: to_device(a, torch.float64, device)
-        de2c, dr, dw, dD = dev(e2c), dev(np.asarray(r)), dev(np.asarray(w)), dev(D)
+        keep = []
+        if connect == "device":
+            n = [len(xi) - 1 for xi in x]
+            nelem = int(np.prod(n))
+            dx = [dev(np.asarray(xi, dtype=np.float64)) for xi in x]
+            keep.extend(dx)
+            de2c = torch.empty(dim * 2 ** dim * nelem, dtype=torch.float64, device=device)
+            detb = torch.empty(2 * dim * nelem, dtype=torch.int64, device=device)
+            dvM = torch.empty(Nfp * 2 * dim * nelem, dtype=torch.int64, device=device)
+            dvP = torch.empty_like(dvM)
+            bnd = None
+            if boundary is not None:
+                b = np.asarray(boundary, dtype=np.int64).reshape(2, dim, order="F")
+                bnd = (C.c_int64 * (2 * dim))(*[int(v) for v in b.ravel(order="F")])
+            check(_lib.lib().cb_brickmesh(
+                dim, N, (C.c_int64 * dim)(*n), (C.c_void_p * dim)(*[t.data_ptr() for t in dx]),
+                (C.c_int * dim)(*[1 if p else 0 for p in periodic]), bnd, _ptr(de2c, torch.float64),
+                _ptr(detb, torch.int64), _ptr(dvM, torch.int64), _ptr(dvP, torch.int64), _stream(stream)))
+            vmapM = vmapP = etb = e2c = None
+        else:
+            cm = connectmesh(*partition(*brickmesh(x, periodic, boundary=boundary)))
+            vmapM, vmapP = mappings(N, cm["elemtoelem"], cm["elemtoface"], cm["elemtoordr"])
+            e2c = np.asarray(cm["elemtocoord"], dtype=np.float64)
+            etb = cm["elemtobndy"]
+            nelem = e2c.shape[2]
+            de2c = dev(e2c)
+            dvM, dvP, detb = dev_i64(vmapM, device), dev_i64(vmapP, device), dev_i64(etb, device)
+        dr, dw, dD = dev(np.asarray(r)), dev(np.asarray(w)), dev(D)
+        keep.extend([dr, dw])
         vgeo = torch.empty(Np * nvg * nelem, dtype=torch.float64, device=device)
         sgeo = torch.empty(nsg * Nfp * 2 * dim * nelem, dtype=torch.float64, device=device)
         check(_lib.lib().cb_computegeometry(dim, N, nelem, _ptr(de2c, torch.float64), float(warp_amp),
                                             _ptr(dr, torch.float64), _ptr(dw, torch.float64),
                                             _ptr(dD, torch.float64), _ptr(vgeo, torch.float64),
                                             _ptr(sgeo, torch.float64), _stream(stream)))
-        mesh = Mesh(dim, N, nelem, None, None, vmapM, vmapP, cm["elemtobndy"], D, np.asarray(r),
-                    np.asarray(w), e2c)
-        return cls(mesh, vgeo, sgeo, dev_i64(vmapM, device), dev_i64(vmapP, device),
-                   dev_i64(cm["elemtobndy"], device), dD)
+        mesh = Mesh(dim, N, nelem, None, None, vmapM, vmapP, etb, D, np.asarray(r), np.asarray(w), e2c)
+        out = cls(mesh, vgeo, sgeo, dvM, dvP, detb, dD)
+        out.elemtocoord = de2c  # device (dim, 2^dim, nelem); with the inputs of the set-up kernels
+        out._keep = keep
+        return out
 
     def coords(self):
         """Node coordinates as device tensors (nelem, Np), one per dimension."""

@@ -224,6 +224,17 @@ __device__ __forceinline__ int face_node(int f, int fn) {
   return a + Nq * (b + Nq * side);
 }
 
+// The same with the order as a run-time value.
+template <int DIM>
+__device__ __forceinline__ int face_node_rt(int Nq, int f, int fn) {
+  const int d0 = f >> 1, side = (f & 1) * (Nq - 1);
+  if (DIM == 2) return d0 == 0 ? side + Nq * fn : fn + Nq * side;
+  const int a = fn % Nq, b = fn / Nq;
+  if (d0 == 0) return side + Nq * (a + Nq * b);
+  if (d0 == 1) return a + Nq * (side + Nq * b);
+  return a + Nq * (b + Nq * side);
+}
+
 // Subtract the face contributions of a node in face order f = 1..nface.
 // FF is [NFACE][NS][EPB*Nfp] (already multiplied by sMJ).
 template <int DIM, int Nq, int EPB, typename T>

@@ -206,6 +206,23 @@ int cb_computegeometry(int dim, int N, int64_t nelem, const double *elemtocoord,
                        const double *D, double *vgeo, double *sgeo,
                        cb_stream_t stream);
 
+/* Cartesian brick mesh and its connectivity on the device: the set-up
+ * sequence brickmesh -> partition -> connectmesh -> mappings of the
+ * reference's drivers (src/mesh.jl:259-317, :499-580, :751-956, :973-1001;
+ * euler3d_set3c.jl:1689-1708) for one rank, with the same element order
+ * (Hilbert code of the centroids, ties by element number) and the same
+ * arrays.  n[d] elements along dimension d between the coordinates x[d]
+ * (device arrays of n[d] + 1 doubles); periodic[d]; boundary (2, dim)
+ * column-major codes of the non-periodic ends (NULL: all 1).  Writes the
+ * device arrays elemtocoord (dim, 2^dim, nelem), elemtobndy (2 dim, nelem),
+ * vmapM and vmapP ((N+1)^(dim-1), 2 dim, nelem, 1-based), nelem = prod n.
+ * Asynchronous on `stream` (its scratch comes from the stream-ordered
+ * allocator). */
+int cb_brickmesh(int dim, int N, const int64_t *n, const double *const *x,
+                 const int *periodic, const int64_t *boundary,
+                 double *elemtocoord, int64_t *elemtobndy, int64_t *vmapM,
+                 int64_t *vmapP, cb_stream_t stream);
+
 /* ---------------------------------------------------------------------- */
 /* Batched LSRK(5,4) over many independent instances (ensembles, serving). */
 /* ---------------------------------------------------------------------- */
