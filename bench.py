@@ -217,8 +217,12 @@ def batched_ensemble(count=512, seed=0, steps=500, device="cuda"):
                        f"{steps} steps each", "instances": count, "steps": steps,
            "host_mesh_setup_s": round(time.time() - t0, 2)}
     finals = {}
+    shapes = sorted({(2, p["N"]) for p in params})
     for prec in (64, 32):
-        ens = B.VortexEnsemble(params, prec, nsteps=steps, cache=cache)
+        t1 = time.time()
+        tuning = B.autotune(prec, shapes)  # stage variant per (dim, N), timed on this GPU
+        out[f"autotune_fp{prec}_s"] = round(time.time() - t1, 2)
+        ens = B.VortexEnsemble(params, prec, nsteps=steps, cache=cache, tuning=tuning)
         torch.cuda.synchronize()
         ens.run(1)  # builds the step graph
         torch.cuda.synchronize()

@@ -273,27 +273,28 @@ class VortexEnsemble:
 # ------------------------------------------------------------------ autotuner
 def autotune(precision: int, shapes, nodes_target: int = 4_000_000, steps: int = 4, repeat: int = 3,
              stream=None) -> dict:
-    """Choose the stage variant (pipelined staging or grouped, and elements
-    per block) of each (dim, N) by timing the batched step on a synthetic
-    instance of that shape with
-    about `nodes_target` nodes: 2-D vortex / 3-D free-stream-plus-Fourier
-    states on periodic meshes.  Returns {(dim, N): variant}."""
+    """Choose the stage variant (pipelined staging at one of several
+    occupancies, or grouped with about 256 / 512 nodes per block) of each
+    (dim, N) by timing the batched step on a synthetic instance of that shape
+    with about `nodes_target` nodes: the 2-D vortex / the 3-D Fourier state
+    on periodic meshes built on the device.  Returns {(dim, N): variant}."""
     torch = _torch()
-    from .ic import fourier_state
+    from . import ic
     best = {}
     for dim, N in shapes:
         Np = (N + 1) ** dim
         n_side = max(2, int(round((nodes_target / Np) ** (1.0 / dim))))
         L = 10.0 if dim == 2 else 2 * np.pi
-        cache = MeshCache()
-        mesh = cache.host(dim, N, n_side, L)
+        dm = DeviceMesh.build(dim, N, (np.linspace(0.0, L, n_side + 1),) * dim, (True,) * dim)
+        X = dm.coords()
         if dim == 2:
-            Q = vortex_state(mesh, 5.0, 5.0, 5.0)
+            f = ic.isentropic_vortex_t(X[0], X[1], 5.0, 5.0, 5.0)
             dt = 1e-4
         else:
-            x, y, z = mesh.coords()
-            Q = np.stack(fourier_state(x, y, z, seed=0, device="cuda"), axis=1)
+            f = ic.fourier_state_t(X[0], X[1], X[2], seed=0)
             dt = 1e-5
+        real = torch.float64 if precision == 64 else torch.float32
+        bm = BatchMesh(dm, precision)
         timings = {}
         for var in VARIANTS:
             b = Batch(precision, 1)
@@ -302,7 +303,8 @@ def autotune(precision: int, shapes, nodes_target: int = 4_000_000, steps: int =
             except Exception:
                 b.close()
                 continue
-            slot = b.add_state(cache.batch_mesh(precision, dim, N, n_side, L), Q, dt, 10 ** 9)
+            Q = ic.device_state(list(f), real)
+            slot = b.add(bm, Q, torch.zeros_like(Q), dt, 10 ** 9)
             b.run(1)  # build the graph, warm up
             ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             ts = []
@@ -316,6 +318,6 @@ def autotune(precision: int, shapes, nodes_target: int = 4_000_000, steps: int =
             timings[var] = min(ts)
             b.release(slot)
             b.close()
-        cache.close()
+        bm.close()
         best[(dim, N)] = min(timings, key=timings.get)
     return best
