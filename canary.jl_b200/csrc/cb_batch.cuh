@@ -206,7 +206,7 @@ __device__ __forceinline__ void stage_group(const BDesc<T> &I, int64_t e0, int n
 // Persistent grouped stage kernel of one shape: the blocks stride over the
 // shape's work list.
 template <int DIM, int Nq, int G, typename T>
-__global__ void __launch_bounds__(BT, sizeof(T) == 4 ? 2 : 1)
+__global__ void __launch_bounds__(BT, 2)
 k_stage_batch(const BHdr *__restrict__ hdr, int stage, PhysT<T> p, T rka, double rkb) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int SID = shape_id(DIM, Nq - 1, 1 + G);
@@ -439,63 +439,76 @@ __device__ __forceinline__ void ns_stage_group(const BDesc<T> &I, const T *__res
 #pragma unroll
     for (int c = 0; c < DIM; ++c) nrm[c] = sg[c];
     const T smj = sg[DIM];
-    T qM[NS], qP[NS], gm[NS][DIM], gp[NS][DIM], vM_[DIM], vP_[DIM];
+    T qM[NS], qP[NS], vM_[DIM], vP_[DIM];
 #pragma unroll
     for (int s = 0; s < NS; ++s) qM[s] = sQ[s * SP + el * Np + vM] + I.qref[s];
-#pragma unroll
-    for (int s = 0; s < NS; ++s)
-#pragma unroll
-      for (int c = 0; c < DIM; ++c) gm[s][c] = gq[vM + Np * (s + NS * (c + (int64_t)DIM * e))];
     const T gM = p.grav != T(0) ? vgeo[vM + Np * (GC + NVG * e)] : T(0);
     const T riM = T(1) / qM[IR];
     const T PM = pressure_ri<DIM, T>(qM, riM, gM, p);
 #pragma unroll
     for (int c = 0; c < DIM; ++c) vM_[c] = qM[c] / qM[IR];
     const int32_t nb = I.nbr[f + NF * e];
+    const int64_t e2 = nb >= 0 ? (int64_t)(nb >> 3) : e;
+    const int vP = nb >= 0 ? face_node<DIM, Nq>(nb & 7, fn) : vM;
     T PP, riP;
     if (nb >= 0) {
-      const int64_t e2 = nb >> 3;
-      const int vP = face_node<DIM, Nq>(nb & 7, fn);
 #pragma unroll
       for (int s = 0; s < NS; ++s) qP[s] = Qin[vP + Np * (s + NS * e2)] + I.qref[s];
-#pragma unroll
-      for (int s = 0; s < NS; ++s)
-#pragma unroll
-        for (int c = 0; c < DIM; ++c) gp[s][c] = gq[vP + Np * (s + NS * (c + (int64_t)DIM * e2))];
       const T gP = p.grav != T(0) ? vgeo[vP + Np * (GC + NVG * e2)] : T(0);
       riP = T(1) / qP[IR];
       PP = pressure_ri<DIM, T>(qP, riP, gP, p);
 #pragma unroll
       for (int c = 0; c < DIM; ++c) vP_[c] = qP[c] / qP[IR];
-    } else {  // reflective wall (nse3d.jl:880-900): mirrored state, velocity and gradients
+    } else {  // reflective wall (nse3d.jl:880-900): mirrored state and velocity
       wall_state<DIM, T>(qM, nrm, qP);
       riP = riM;
       PP = PM;
-#pragma unroll
-      for (int s = 0; s < NS; ++s) {
-        T sn = nrm[0] * gm[s][0] + nrm[1] * gm[s][1];
-        if (DIM == 3) sn = sn + nrm[2] * gm[s][2];
-#pragma unroll
-        for (int c = 0; c < DIM; ++c) gp[s][c] = gm[s][c] - T(2) * sn * nrm[c];
-      }
       T un = nrm[0] * vM_[0] + nrm[1] * vM_[1];
       if (DIM == 3) un = un + nrm[2] * vM_[2];
 #pragma unroll
       for (int c = 0; c < DIM; ++c) vP_[c] = vM_[c] - T(2) * un * nrm[c];
-#pragma unroll
-      for (int c = 0; c < DIM; ++c) gp[IE][c] = gm[IE][c];
     }
     T out[NS];
     rusanov_n<DIM, T>(qM, riM, PM, qP, riP, PP, nrm, p, out);
-    T fM[NS][DIM], fP[NS][DIM];
-    visc_flux<DIM, T>(gm, vM_, p, fM);
-    visc_flux<DIM, T>(gp, vP_, p, fP);
+    // n · (F_visc⁻ + F_visc⁺), one side at a time (fewer live registers)
+    T av[NS];
+    {
+      T g[NS][DIM], fv[NS][DIM];
 #pragma unroll
-    for (int s = 0; s < NS; ++s) {
-      T a = nrm[0] * (fM[s][0] + fP[s][0]) + nrm[1] * (fM[s][1] + fP[s][1]);
-      if (DIM == 3) a = a + nrm[2] * (fM[s][2] + fP[s][2]);
-      FF[(f * NS + s) * FS + el * Nfp + fn] = smj * out[s] - p.visc * (smj * (T(0.5) * a));
+      for (int s = 0; s < NS; ++s)
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) g[s][c] = gq[vM + Np * (s + NS * (c + (int64_t)DIM * e))];
+      visc_flux<DIM, T>(g, vM_, p, fv);
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        av[s] = nrm[0] * fv[s][0] + nrm[1] * fv[s][1];
+        if (DIM == 3) av[s] = av[s] + nrm[2] * fv[s][2];
+      }
+      if (nb >= 0) {
+#pragma unroll
+        for (int s = 0; s < NS; ++s)
+#pragma unroll
+          for (int c = 0; c < DIM; ++c) g[s][c] = gq[vP + Np * (s + NS * (c + (int64_t)DIM * e2))];
+      } else {  // mirrored gradients, the temperature gradient copied from the interior
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+          if (s == IE) continue;
+          T sn = nrm[0] * g[s][0] + nrm[1] * g[s][1];
+          if (DIM == 3) sn = sn + nrm[2] * g[s][2];
+#pragma unroll
+          for (int c = 0; c < DIM; ++c) g[s][c] = g[s][c] - T(2) * sn * nrm[c];
+        }
+      }
+      visc_flux<DIM, T>(g, vP_, p, fv);
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        T b = nrm[0] * fv[s][0] + nrm[1] * fv[s][1];
+        if (DIM == 3) b = b + nrm[2] * fv[s][2];
+        av[s] = av[s] + b;
+      }
     }
+#pragma unroll
+    for (int s = 0; s < NS; ++s) FF[(f * NS + s) * FS + el * Nfp + fn] = smj * out[s] - p.visc * (smj * (T(0.5) * av[s]));
   }
   __syncthreads();
   bool bad = false;
@@ -522,7 +535,7 @@ __device__ __forceinline__ void ns_stage_group(const BDesc<T> &I, const T *__res
 
 // Persistent viscous passes of one shape (the grouped variant's work list).
 template <int DIM, int Nq, typename T, bool GRAD>
-__global__ void __launch_bounds__(BT, sizeof(T) == 4 ? 2 : 1)
+__global__ void __launch_bounds__(BT, 2)
 k_ns_batch(const BHdr *__restrict__ hdr, int stage, PhysT<T> p, T rka, double rkb) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int SID = shape_id(DIM, Nq - 1, 1);
@@ -556,7 +569,7 @@ __device__ __forceinline__ void prefetch_l2(const void *p, size_t bytes) {
 }
 
 template <int DIM, int Nq, typename T, bool GRAD>
-__global__ void __launch_bounds__(BT, sizeof(T) == 4 ? 2 : 1)
+__global__ void __launch_bounds__(BT, 2)
 k_ns_mesh(BDesc<T> I, T *gq, int64_t nelem, PhysT<T> p, T rka, T rkbdt) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   using C = BCfg<DIM, Nq, 0>;
