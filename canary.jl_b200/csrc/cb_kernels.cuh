@@ -301,7 +301,9 @@ __global__ void k_build_nbr(int32_t *__restrict__ nbr,
                             const int64_t *__restrict__ vmapM,
                             const int64_t *__restrict__ vmapP,
                             const int64_t *__restrict__ elemtobndy,
-                            int64_t nelem, unsigned *status) {
+                            int64_t nelem, int64_t nall, unsigned *status) {
+  // nall: elements a neighbour may be (nelem, plus the ghost elements that a
+  // partitioned solve appends after its own)
   using C = Cfg<DIM, Nq>;
   constexpr int Np = C::Np, Nfp = C::Nfp, NF = C::NFACE;
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -325,7 +327,7 @@ __global__ void k_build_nbr(int32_t *__restrict__ nbr,
         for (int fn = 0; fn < Nfp; ++fn) m &= vp[fn] == Np * e2 + face_node<DIM, Nq>(g, fn) + 1;
         if (m) { f2 = g; break; }
       }
-    ok &= f2 >= 0 && e2 >= 0 && e2 < nelem && e2 < (1ll << 28);
+    ok &= f2 >= 0 && e2 >= 0 && e2 < nall && e2 < (1ll << 28);
     nbr[t] = ok ? (int32_t)((e2 << 3) | f2) : NBR_WALL;
   } else {
     atomicOr(status, ST_BC);
@@ -842,7 +844,14 @@ struct Launch {
                                const int64_t *bnd, int64_t nelem, unsigned *status,
                                cudaStream_t st) {
     const int64_t n = nelem * C::NFACE;
-    k_build_nbr<DIM, Nq><<<(int)((n + 255) / 256), 256, 0, st>>>(nbr, vmapM, vmapP, bnd, nelem, status);
+    k_build_nbr<DIM, Nq><<<(int)((n + 255) / 256), 256, 0, st>>>(nbr, vmapM, vmapP, bnd, nelem, nelem, status);
+    return cudaGetLastError();
+  }
+  static cudaError_t build_nbr_ghost(int32_t *nbr, const int64_t *vmapM, const int64_t *vmapP,
+                                     const int64_t *bnd, int64_t nelem, int64_t nall, unsigned *status,
+                                     cudaStream_t st) {
+    const int64_t n = nelem * C::NFACE;
+    k_build_nbr<DIM, Nq><<<(int)((n + 255) / 256), 256, 0, st>>>(nbr, vmapM, vmapP, bnd, nelem, nall, status);
     return cudaGetLastError();
   }
   static cudaError_t volume_grad(T *rhs, const T *Q, const T *vgeo, const T *D, int64_t nelem,

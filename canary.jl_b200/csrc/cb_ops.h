@@ -22,6 +22,9 @@ struct Ops {
                        const PhysT<T> &, const Offs<T, 5> &, T, T, unsigned *, cudaStream_t);
   cudaError_t (*build_nbr)(int32_t *, const int64_t *, const int64_t *, const int64_t *, int64_t,
                            unsigned *, cudaStream_t);
+  // the same with neighbours allowed up to a total element count (ghosts)
+  cudaError_t (*build_nbr_ghost)(int32_t *, const int64_t *, const int64_t *, const int64_t *, int64_t,
+                                 int64_t, unsigned *, cudaStream_t);
   cudaError_t (*volume_grad)(T *, const T *, const T *, const T *, int64_t, const PhysT<T> &, cudaStream_t);
   cudaError_t (*flux_grad)(T *, const T *, const T *, const T *, int64_t, const int64_t *,
                            const int64_t *, const int64_t *, const PhysT<T> &, unsigned *, cudaStream_t);

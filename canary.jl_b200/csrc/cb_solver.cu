@@ -47,6 +47,8 @@ struct cb_solver {
   cudaGraphExec_t exec = nullptr;
   double graph_dt = NAN;
   double qref[5] = {0, 0, 0, 0, 0};  // stored state = Q - qref
+  int64_t nghost = 0;  // ghost elements after the nelem own ones in Q and the twin
+  int cur = 0;         // stage API: the current state is in Q (0) or in the twin (1)
 };
 
 namespace {
@@ -156,6 +158,61 @@ int capture(cb_solver *s, double dt) {
   return CB_OK;
 }
 
+int solver_create(cb_solver **out, int dim, int N, int precision, int64_t nelem, int64_t nghost, void *Q,
+                  void *rhs, const double *vgeo, const double *sgeo, const int64_t *vmapM, const int64_t *vmapP,
+                  const int64_t *elemtobndy, const double *D, const cb_phys *phys, cb_stream_t stream);
+
+// state bytes of the nelem own elements
+size_t state_bytes(const cb_solver *s) {
+  const int Nq = s->N + 1;
+  const int64_t Np = s->dim == 2 ? (int64_t)Nq * Nq : (int64_t)Nq * Nq * Nq;
+  return (s->prec == 64 ? 8 : 4) * (size_t)Np * (s->dim == 2 ? 4 : 5) * s->nelem;
+}
+
+// bring the state back into the caller's Q after an odd number of stages
+cudaError_t settle(cb_solver *s) {
+  if (!s->cur) return cudaSuccess;
+  s->cur = 0;
+  return cudaMemcpyAsync(s->Q, s->Qalt, state_bytes(s), cudaMemcpyDeviceToDevice, s->stream);
+}
+
+// one RK stage from the current buffer into the other
+template <typename T>
+cudaError_t enqueue_one(cb_solver *s, int st, double dt) {
+  const Ops<T> *o = ops<T>(s);
+  const PhysT<T> p(Phys{s->phys.gamma, s->phys.R_gas, s->phys.c_p, s->phys.c_v, s->phys.gravity,
+                        s->phys.Pr, s->phys.lambda, s->phys.visc});
+  T *a = (T *)(s->cur ? s->Qalt : s->Q), *b = (T *)(s->cur ? s->Q : s->Qalt);
+  if (fused_visc(s)) {
+    BDesc<T> I{};
+    I.Q[0] = a;
+    I.Q[1] = b;
+    I.rhs = (T *)s->rhs;
+    I.vgeo = (const T *)s->vgeo;
+    I.sgeo = (const T *)s->sgeo;
+    I.D = (const T *)s->D;
+    I.nbr = s->nbr;
+    I.status = s->status;
+    I.dt = dt;
+    for (int k = 0; k < 5; ++k) I.qref[k] = T(s->qref[k]);
+    cudaError_t e = o->ns_pass(0, I, (T *)s->gradQ, s->nelem, p, T(0), T(0), s->stream);
+    return e != cudaSuccess ? e : o->ns_pass(1, I, (T *)s->gradQ, s->nelem, p, T(RKA[(st + 1) % 5]), T(RKB[st] * dt), s->stream);
+  }
+  Offs<T, 5> q5;
+  for (int k = 0; k < 5; ++k) q5.v[k] = T(s->qref[k]);
+  return o->stage(a, b, (T *)s->rhs, (const T *)s->vgeo, (const T *)s->sgeo, s->nbr, (const T *)s->D, s->nelem, p,
+                  q5, T(RKA[(st + 1) % 5]), T(RKB[st] * dt), s->status, s->stream);
+}
+
+// Copy whole elements: gather `n` elements listed in `idx` (device int64) of
+// `src` into the contiguous `dst`.
+template <typename T>
+__global__ void k_pack(const T *__restrict__ src, const int64_t *__restrict__ idx, int64_t n, int64_t ew,
+                       T *__restrict__ dst) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n * ew; t += (int64_t)gridDim.x * blockDim.x)
+    dst[t] = src[idx[t / ew] * ew + t % ew];
+}
+
 }  // namespace
 
 extern "C" {
@@ -164,6 +221,75 @@ int cb_solver_create(cb_solver **out, int dim, int N, int precision, int64_t nel
                      void *rhs, const double *vgeo, const double *sgeo, const int64_t *vmapM,
                      const int64_t *vmapP, const int64_t *elemtobndy, const double *D,
                      const cb_phys *phys, cb_stream_t stream) {
+  return solver_create(out, dim, N, precision, nelem, 0, Q, rhs, vgeo, sgeo, vmapM, vmapP, elemtobndy, D, phys,
+                       stream);
+}
+
+int cb_solver_create_ghosted(cb_solver **out, int dim, int N, int precision, int64_t nelem, int64_t nghost,
+                             void *Q, void *rhs, const double *vgeo, const double *sgeo, const int64_t *vmapM,
+                             const int64_t *vmapP, const int64_t *elemtobndy, const double *D,
+                             const cb_phys *phys, cb_stream_t stream) {
+  if (nghost < 0) return solver_fail(CB_ERR_ARG, "cb_solver_create_ghosted: nghost must be >= 0");
+  if (phys && phys->visc > 0)
+    return solver_fail(CB_ERR_UNSUPPORTED, "cb_solver_create_ghosted: the partitioned form is inviscid");
+  return solver_create(out, dim, N, precision, nelem, nghost, Q, rhs, vgeo, sgeo, vmapM, vmapP, elemtobndy, D,
+                       phys, stream);
+}
+
+int cb_solver_stage(cb_solver *s, int stage, double dt, void **next_in) {
+  if (!s || stage < 0 || stage > 4) return solver_fail(CB_ERR_ARG, "cb_solver_stage: bad arguments");
+  if (!pingpong(s)) return solver_fail(CB_ERR_UNSUPPORTED, "cb_solver_stage: this viscous order has no stage form");
+  const cudaError_t e = s->prec == 64 ? enqueue_one<double>(s, stage, dt) : enqueue_one<float>(s, stage, dt);
+  if (e != cudaSuccess) return solver_fail(CB_ERR_CUDA, "cb_solver_stage: %s", cudaGetErrorString(e));
+  s->cur ^= 1;
+  if (next_in) *next_in = s->cur ? s->Qalt : s->Q;
+  return CB_OK;
+}
+
+int cb_solver_current(const cb_solver *s, void **state) {
+  if (!s || !state) return solver_fail(CB_ERR_ARG, "cb_solver_current: null argument");
+  *state = s->cur ? s->Qalt : s->Q;
+  return CB_OK;
+}
+
+int cb_solver_settle(cb_solver *s) {
+  if (!s) return solver_fail(CB_ERR_ARG, "cb_solver_settle: null solver");
+  const cudaError_t e = settle(s);
+  return e == cudaSuccess ? CB_OK : solver_fail(CB_ERR_CUDA, "cb_solver_settle: %s", cudaGetErrorString(e));
+}
+
+int cb_solver_pack(cb_solver *s, const int64_t *elems, int64_t n, void *buf) {
+  if (!s || n < 0 || (n && (!elems || !buf))) return solver_fail(CB_ERR_ARG, "cb_solver_pack: bad arguments");
+  if (!n) return CB_OK;
+  const int Nq = s->N + 1;
+  const int64_t ew = (s->dim == 2 ? (int64_t)Nq * Nq * 4 : (int64_t)Nq * Nq * Nq * 5);
+  const int grid = (int)std::min<int64_t>((n * ew + 255) / 256, 148 * 16);
+  const void *src = s->cur ? s->Qalt : s->Q;
+  if (s->prec == 64)
+    k_pack<double><<<grid, 256, 0, s->stream>>>((const double *)src, elems, n, ew, (double *)buf);
+  else
+    k_pack<float><<<grid, 256, 0, s->stream>>>((const float *)src, elems, n, ew, (float *)buf);
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? CB_OK : solver_fail(CB_ERR_CUDA, "cb_solver_pack: %s", cudaGetErrorString(e));
+}
+
+int cb_solver_unpack(cb_solver *s, const void *buf, int64_t first, int64_t n) {
+  if (!s || first < 0 || n < 0 || first + n > s->nghost || (n && !buf))
+    return solver_fail(CB_ERR_ARG, "cb_solver_unpack: ghost range outside 0..%lld", (long long)s->nghost);
+  if (!n) return CB_OK;
+  const size_t ew = state_bytes(s) / (size_t)s->nelem;
+  char *dst = (char *)(s->cur ? s->Qalt : s->Q) + ew * (size_t)(s->nelem + first);
+  const cudaError_t e = cudaMemcpyAsync(dst, buf, ew * (size_t)n, cudaMemcpyDeviceToDevice, s->stream);
+  return e == cudaSuccess ? CB_OK : solver_fail(CB_ERR_CUDA, "cb_solver_unpack: %s", cudaGetErrorString(e));
+}
+
+}  // extern "C"
+
+namespace {
+
+int solver_create(cb_solver **out, int dim, int N, int precision, int64_t nelem, int64_t nghost, void *Q,
+                  void *rhs, const double *vgeo, const double *sgeo, const int64_t *vmapM, const int64_t *vmapP,
+                  const int64_t *elemtobndy, const double *D, const cb_phys *phys, cb_stream_t stream) {
   if (!out || !Q || !rhs || !vgeo || !sgeo || !vmapM || !vmapP || !elemtobndy || !D || !phys)
     return solver_fail(CB_ERR_ARG, "cb_solver_create: null pointer argument");
   if (dim != 2 && dim != 3) return solver_fail(CB_ERR_ARG, "dim must be 2 or 3");
@@ -182,6 +308,7 @@ int cb_solver_create(cb_solver **out, int dim, int N, int precision, int64_t nel
   s->vmapP = vmapP;
   s->bnd = elemtobndy;
   s->phys = *phys;
+  s->nghost = nghost;
   cudaGetDevice(&s->device);
   const int Nq = N + 1;
   const int64_t Np = dim == 2 ? (int64_t)Nq * Nq : (int64_t)Nq * Nq * Nq;
@@ -216,7 +343,8 @@ int cb_solver_create(cb_solver **out, int dim, int N, int precision, int64_t nel
     }
   }
   if (pingpong(s)) {
-    if ((e = cudaMalloc(&s->Qalt, w * (size_t)Np * ns * nelem)) != cudaSuccess) return bail(CB_ERR_NOMEM, "state twin");
+    if ((e = cudaMalloc(&s->Qalt, w * (size_t)Np * ns * (nelem + nghost))) != cudaSuccess)
+      return bail(CB_ERR_NOMEM, "state twin");
     if ((e = cudaMalloc(&s->nbr, sizeof(int32_t) * nface * nelem)) != cudaSuccess) return bail(CB_ERR_NOMEM, "neighbours");
   }
   if (precision == 64) {
@@ -239,7 +367,8 @@ int cb_solver_create(cb_solver **out, int dim, int N, int precision, int64_t nel
   if (e != cudaSuccess) return bail(CB_ERR_CUDA, "kernel attributes");
   if (pingpong(s)) {
     const Ops<double> *o = ops<double>(s);
-    if ((e = o->build_nbr(s->nbr, vmapM, vmapP, elemtobndy, nelem, s->status, s->stream)) != cudaSuccess)
+    if ((e = o->build_nbr_ghost(s->nbr, vmapM, vmapP, elemtobndy, nelem, nelem + nghost, s->status, s->stream)) !=
+        cudaSuccess)
       return bail(CB_ERR_CUDA, "neighbour table");
   }
   unsigned h = 0;
@@ -258,10 +387,16 @@ int cb_solver_create(cb_solver **out, int dim, int N, int precision, int64_t nel
   return CB_OK;
 }
 
+}  // namespace
+
+extern "C" {
+
 int cb_lsrk_run(cb_solver *s, int64_t nsteps, double dt) {
   if (!s) return solver_fail(CB_ERR_ARG, "null solver");
   if (nsteps < 0) return solver_fail(CB_ERR_ARG, "nsteps must be >= 0");
   if (nsteps == 0) return CB_OK;
+  cudaError_t e0 = settle(s);  // a state left in the twin by the stage API
+  if (e0 != cudaSuccess) return solver_fail(CB_ERR_CUDA, "state copy: %s", cudaGetErrorString(e0));
   const int64_t per_graph = pingpong(s) ? 2 : 1;
   const int64_t reps = nsteps / per_graph, rem = nsteps % per_graph;
   cudaError_t e;
@@ -292,9 +427,10 @@ int cb_solver_sums(cb_solver *s, double *out_host) {
   const int Np = s->dim == 2 ? Nq * Nq : Nq * Nq * Nq;
   Offs<double, 5> q5;
   for (int k = 0; k < 5; ++k) q5.v[k] = s->qref[k];
+  const void *Qc = s->cur ? s->Qalt : s->Q;  // the current state
   cudaError_t e = s->prec == 64
-                      ? ops<double>(s)->cons_sums((const double *)s->Q, (const double *)s->vgeo, s->nelem, Np, q5, s->part, s->part_blocks, s->stream)
-                      : ops<float>(s)->cons_sums((const float *)s->Q, (const float *)s->vgeo, s->nelem, Np, q5, s->part, s->part_blocks, s->stream);
+                      ? ops<double>(s)->cons_sums((const double *)Qc, (const double *)s->vgeo, s->nelem, Np, q5, s->part, s->part_blocks, s->stream)
+                      : ops<float>(s)->cons_sums((const float *)Qc, (const float *)s->vgeo, s->nelem, Np, q5, s->part, s->part_blocks, s->stream);
   if (e != cudaSuccess) return solver_fail(CB_ERR_CUDA, "sums launch: %s", cudaGetErrorString(e));
   std::string buf(sizeof(double) * 4 * ns * s->part_blocks, '\0');
   double *h = (double *)&buf[0];

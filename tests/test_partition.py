@@ -1,0 +1,59 @@
+"""Element-partitioned solve (cb_solver_create_ghosted and the stage API):
+several parts of one mesh advanced in lock step in this process, ghosts moved
+by device copies, give the unpartitioned single-mesh result bit for bit —
+every element's arithmetic is the same.  The inter-rank transport is
+covered on the host (tests/test_partition_host.py, gloo)."""
+import math
+
+import numpy as np
+import pytest
+
+from conftest import cuda_available
+from dg_cases import oracle_run, relerr_fields
+from canary_b200 import dg, ic
+from canary_b200 import partition as P
+from canary_b200.metric import warp_sinusoidal
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not cuda_available(), reason="needs a CUDA GPU")]
+
+
+def cube(N, n, walls=False):
+    m = dg.build_mesh(3, N, (np.linspace(0, 2 * math.pi, n + 1),) * 3, (True, True, not walls),
+                      meshwarp=lambda X: warp_sinusoidal(X, 0.05))
+    x, y, z = m.coords()
+    Q = np.zeros((m.Np, 5, m.nelem), order="F")
+    for c, v in enumerate(ic.fourier_state(x, y, z, seed=N)):
+        Q[:, c] = v
+    return m, Q, 0.5 * ic.fourier_dt(Q, N, h=2 * math.pi / n)
+
+
+def square(N, n):
+    m = dg.build_mesh(2, N, (np.linspace(0, 10, n + 1),) * 2, (True, False))
+    x, y = m.coords()
+    Q = np.zeros((m.Np, 4, m.nelem), order="F")
+    for c, v in enumerate(ic.isentropic_vortex(x, y, 3.0, 5.0, 5.0)):
+        Q[:, c] = v
+    return m, Q, 0.002
+
+
+@pytest.mark.parametrize("case,world", [("cube3", 2), ("cube3", 5), ("cube4w", 3), ("square", 4)])
+@pytest.mark.parametrize("precision", [64, 32])
+def test_parts_equal_single_mesh(case, world, precision):
+    import torch
+    m, Q, dt = {"cube3": lambda: cube(3, 4), "cube4w": lambda: cube(4, 3, walls=True),
+                "square": lambda: square(5, 6)}[case]()
+    k = 3
+    single = dg.LSRK.for_state(dg.DeviceMesh.upload(m), Q, precision)
+    single.run(k, dt)
+    ref = single.state()
+    single.close()
+    stream = torch.cuda.Stream()
+    parts = [P.GhostedLSRK(m, P.plan(m, r, world), Q, precision, stream=stream) for r in range(world)]
+    P.run_parts(parts, k, dt)
+    got = np.concatenate([p.state() for p in parts], axis=2)
+    for p in parts:
+        p.close()
+    assert np.array_equal(got, ref)
+    if precision == 64:
+        assert max(relerr_fields(got, oracle_run(m, Q, dt, k))) < 1e-12
