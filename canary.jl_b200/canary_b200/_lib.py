@@ -25,7 +25,7 @@ EXPORTS = (
     "cb_volume_grad", "cb_flux_grad", "cb_update_gradQ", "cb_volume_div", "cb_flux_div",
     "cb_solver_create", "cb_lsrk_run", "cb_solver_set_offset", "cb_solver_sums",
     "cb_solver_destroy", "cb_solver_status_async", "cb_lsrk_stage_noalloc",
-    "cb_solver_create_ghosted", "cb_solver_stage", "cb_solver_current", "cb_solver_settle",
+    "cb_solver_create_ghosted", "cb_solver_stage", "cb_solver_stage_pass", "cb_solver_current", "cb_solver_settle",
     "cb_solver_pack", "cb_solver_unpack",
     "cb_computegeometry", "cb_brickmesh", "cb_mesh_create", "cb_mesh_affine", "cb_mesh_destroy",
     "cb_batch_create", "cb_batch_set_variant", "cb_batch_get_variant", "cb_batch_set_affine",
@@ -86,10 +86,11 @@ def lib() -> C.CDLL:
     L.cb_solver_create_ghosted.argtypes = [C.POINTER(vp), C.c_int, C.c_int, C.c_int, i64, i64, vp, vp, vp, vp,
                                            vp, vp, vp, vp, phys_p, vp]
     L.cb_solver_stage.argtypes = [vp, C.c_int, dbl, C.POINTER(vp)]
+    L.cb_solver_stage_pass.argtypes = [vp, C.c_int, dbl, C.c_int, C.POINTER(vp)]
     L.cb_solver_current.argtypes = [vp, C.POINTER(vp)]
     L.cb_solver_settle.argtypes = [vp]
-    L.cb_solver_pack.argtypes = [vp, vp, i64, vp]
-    L.cb_solver_unpack.argtypes = [vp, vp, i64, i64]
+    L.cb_solver_pack.argtypes = [vp, C.c_int, vp, i64, vp]
+    L.cb_solver_unpack.argtypes = [vp, C.c_int, vp, i64, i64]
     L.cb_lsrk_stage_noalloc.argtypes = [C.c_int, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp, i64,
                                         phys_p, dbl, dbl, dbl, vp, vp]
     L.cb_computegeometry.argtypes = [C.c_int, C.c_int, i64, vp, dbl, vp, vp, vp, vp, vp, vp]

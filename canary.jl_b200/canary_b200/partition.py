@@ -18,11 +18,12 @@ euler2d_set2c.jl:529-594, :707-735).  Here:
   torch.distributed point-to-point operations (NCCL between GPUs; any
   backend whose tensors the solver can read);
 * `PartitionedLSRK` runs the LSRK steps: exchange, then stage, five times a
-  step.
+  step; the viscous form (orders with the fused passes) exchanges the state,
+  runs the gradient pass, exchanges the gradient, then runs the stage pass.
 
 Every element's arithmetic is the single-mesh solver's, so the partitioned
 result equals the unpartitioned one bit for bit (tests/test_partition.py
-checks this with several partitions in one process).  Inviscid form.
+checks this with several partitions in one process).
 """
 from __future__ import annotations
 
@@ -113,6 +114,8 @@ class GhostedLSRK:
         self.phys = phys or make_phys()
         ns, Np = nstate(mesh.dim), mesh.Np
         self.ew = ns * Np
+        self.visc = self.phys.visc > 0
+        self.widths = (self.ew, self.ew * mesh.dim)  # element width of the state and of its gradient
         Q = np.asarray(Q, dtype=np.float64)
         if offset is None:
             offset = Q.mean(axis=(0, 2)) if precision == 32 else np.zeros(ns)
@@ -136,20 +139,27 @@ class GhostedLSRK:
         arr = (C.c_double * 5)(*([float(v) for v in self.offset] + [0.0] * (5 - ns)))
         check(_lib.lib().cb_solver_set_offset(self._h, arr))
 
-    def stage(self, st: int, dt: float) -> None:
-        """One RK stage (0..4) of the own elements; the ghosts of the state it
-        reads must have been filled."""
+    def stage(self, st: int, dt: float, pass_: int = None) -> None:
+        """RK stage st (0..4) of the own elements, or one pass of it (0: the
+        viscous gradient, 1: the stage); the ghosts of what it reads must have
+        been filled."""
         nxt = C.c_void_p()
-        check(_lib.lib().cb_solver_stage(self._h, int(st), float(dt), C.byref(nxt)))
+        if pass_ is None:
+            check(_lib.lib().cb_solver_stage(self._h, int(st), float(dt), C.byref(nxt)))
+        else:
+            check(_lib.lib().cb_solver_stage_pass(self._h, int(st), float(dt), int(pass_), C.byref(nxt)))
 
-    def pack(self, idx, buf) -> None:
-        """Gather own elements idx (device int64) of the current state into buf."""
-        check(_lib.lib().cb_solver_pack(self._h, C.c_void_p(idx.data_ptr()), int(idx.numel()),
+    def pack(self, idx, buf, what: int = 0) -> None:
+        """Gather own elements idx (device int64) of the current state (what =
+        0) or of the gradient (1) into buf."""
+        check(_lib.lib().cb_solver_pack(self._h, int(what), C.c_void_p(idx.data_ptr()), int(idx.numel()),
                                         C.c_void_p(buf.data_ptr())))
 
-    def unpack(self, buf, first: int, count: int) -> None:
-        """Store count received elements from buf as ghosts first.. of the current state."""
-        check(_lib.lib().cb_solver_unpack(self._h, C.c_void_p(buf.data_ptr()), int(first), int(count)))
+    def unpack(self, buf, first: int, count: int, what: int = 0) -> None:
+        """Store count received elements from buf as ghosts first.. of the
+        current state (what = 0) or of the gradient (1)."""
+        check(_lib.lib().cb_solver_unpack(self._h, int(what), C.c_void_p(buf.data_ptr()), int(first),
+                                          int(count)))
 
     def state(self) -> np.ndarray:
         """Full FP64 state of the own elements (Np, nstate, nloc) on the host."""
@@ -173,31 +183,36 @@ class GhostedLSRK:
 
 class Exchange:
     """Ghost exchange of one rank with torch.distributed point-to-point
-    operations.  `part` provides pack(idx, buf) / unpack(buf, first, count)
-    and the element width `ew`; buffers live on `device` with `dtype`."""
+    operations.  `part` provides pack(idx, buf, what) / unpack(buf, first,
+    count, what) and the element widths `widths` of what = 0 (state) and 1
+    (gradient); buffers live on `device` with `dtype`."""
 
     def __init__(self, p: PartPlan, part, dtype, device, group=None):
         torch = _torch()
         self.part, self.group = part, group
+        wmax = max(part.widths)
         self.sends = [(q, torch.as_tensor(idx, dtype=torch.int64, device=device),
-                       torch.empty(len(idx) * part.ew, dtype=dtype, device=device)) for q, idx in p.send]
-        self.recvs = [(q, first, n, torch.empty(n * part.ew, dtype=dtype, device=device)) for q, first, n in p.recv]
+                       torch.empty(len(idx) * wmax, dtype=dtype, device=device)) for q, idx in p.send]
+        self.recvs = [(q, first, n, torch.empty(n * wmax, dtype=dtype, device=device)) for q, first, n in p.recv]
 
-    def fill(self) -> None:
+    def fill(self, what: int = 0) -> None:
         import torch.distributed as dist
-        for q, idx, buf in self.sends:
-            self.part.pack(idx, buf)
+        w = self.part.widths[what]
+        sends = [(q, idx, buf[:len(idx) * w]) for q, idx, buf in self.sends]
+        recvs = [(q, first, n, buf[:n * w]) for q, first, n, buf in self.recvs]
+        for q, idx, buf in sends:
+            self.part.pack(idx, buf, what)
         if dist.get_backend(self.group) == "nccl":  # one NCCL group for all peers
-            ops = [dist.P2POp(dist.isend, buf, q, self.group) for q, _, buf in self.sends]
-            ops += [dist.P2POp(dist.irecv, buf, q, self.group) for q, _, _, buf in self.recvs]
+            ops = [dist.P2POp(dist.isend, buf, q, self.group) for q, _, buf in sends]
+            ops += [dist.P2POp(dist.irecv, buf, q, self.group) for q, _, _, buf in recvs]
             reqs = dist.batch_isend_irecv(ops) if ops else []
         else:
-            reqs = [dist.isend(buf, q, self.group) for q, _, buf in self.sends]
-            reqs += [dist.irecv(buf, q, self.group) for q, _, _, buf in self.recvs]
+            reqs = [dist.isend(buf, q, self.group) for q, _, buf in sends]
+            reqs += [dist.irecv(buf, q, self.group) for q, _, _, buf in recvs]
         for r in reqs:
             r.wait()
-        for q, first, n, buf in self.recvs:
-            self.part.unpack(buf, first, n)
+        for q, first, n, buf in recvs:
+            self.part.unpack(buf, first, n, what)
 
 
 class PartitionedLSRK:
@@ -215,8 +230,13 @@ class PartitionedLSRK:
         with torch.cuda.stream(self.part.stream):
             for _ in range(nsteps):
                 for st in range(5):
-                    self.exchange.fill()
-                    self.part.stage(st, dt)
+                    self.exchange.fill(0)
+                    if self.part.visc:
+                        self.part.stage(st, dt, 0)
+                        self.exchange.fill(1)
+                        self.part.stage(st, dt, 1)
+                    else:
+                        self.part.stage(st, dt)
 
     def state(self) -> np.ndarray:
         return self.part.state()
@@ -235,14 +255,26 @@ def run_parts(parts, nsteps: int, dt: float) -> None:
         for q, first, n in part.plan.recv:
             idx = dict(parts[q].plan.send)[r]
             bufs[(r, q)] = (torch.as_tensor(idx, dtype=torch.int64, device=part.Q.device),
-                            torch.empty(n * part.ew, dtype=part.real, device=part.Q.device), first, n)
+                            torch.empty(n * max(part.widths), dtype=part.real, device=part.Q.device), first, n)
+
+    def fill(what):
+        for r, part in enumerate(parts):
+            for q, first, n in part.plan.recv:
+                idx, buf, first, n = bufs[(r, q)]
+                b = buf[:n * part.widths[what]]
+                parts[q].pack(idx, b, what)
+                part.unpack(b, first, n, what)
+
     with torch.cuda.stream(parts[0].stream):
         for _ in range(nsteps):
             for st in range(5):
-                for r, part in enumerate(parts):
-                    for q, first, n in part.plan.recv:
-                        idx, buf, first, n = bufs[(r, q)]
-                        parts[q].pack(idx, buf)
-                        part.unpack(buf, first, n)
-                for part in parts:
-                    part.stage(st, dt)
+                fill(0)
+                if parts[0].visc:
+                    for part in parts:
+                        part.stage(st, dt, 0)
+                    fill(1)
+                    for part in parts:
+                        part.stage(st, dt, 1)
+                else:
+                    for part in parts:
+                        part.stage(st, dt)

@@ -176,9 +176,11 @@ cudaError_t settle(cb_solver *s) {
   return cudaMemcpyAsync(s->Q, s->Qalt, state_bytes(s), cudaMemcpyDeviceToDevice, s->stream);
 }
 
-// one RK stage from the current buffer into the other
+// one pass of an RK stage: pass 0 the viscous gradient of the current state
+// (nothing for the inviscid form), pass 1 the stage from the current buffer
+// into the other
 template <typename T>
-cudaError_t enqueue_one(cb_solver *s, int st, double dt) {
+cudaError_t enqueue_pass(cb_solver *s, int st, double dt, int pass) {
   const Ops<T> *o = ops<T>(s);
   const PhysT<T> p(Phys{s->phys.gamma, s->phys.R_gas, s->phys.c_p, s->phys.c_v, s->phys.gravity,
                         s->phys.Pr, s->phys.lambda, s->phys.visc});
@@ -195,9 +197,10 @@ cudaError_t enqueue_one(cb_solver *s, int st, double dt) {
     I.status = s->status;
     I.dt = dt;
     for (int k = 0; k < 5; ++k) I.qref[k] = T(s->qref[k]);
-    cudaError_t e = o->ns_pass(0, I, (T *)s->gradQ, s->nelem, p, T(0), T(0), s->stream);
-    return e != cudaSuccess ? e : o->ns_pass(1, I, (T *)s->gradQ, s->nelem, p, T(RKA[(st + 1) % 5]), T(RKB[st] * dt), s->stream);
+    return pass == 0 ? o->ns_pass(0, I, (T *)s->gradQ, s->nelem, p, T(0), T(0), s->stream)
+                     : o->ns_pass(1, I, (T *)s->gradQ, s->nelem, p, T(RKA[(st + 1) % 5]), T(RKB[st] * dt), s->stream);
   }
+  if (pass == 0) return cudaSuccess;
   Offs<T, 5> q5;
   for (int k = 0; k < 5; ++k) q5.v[k] = T(s->qref[k]);
   return o->stage(a, b, (T *)s->rhs, (const T *)s->vgeo, (const T *)s->sgeo, s->nbr, (const T *)s->D, s->nelem, p,
@@ -230,20 +233,25 @@ int cb_solver_create_ghosted(cb_solver **out, int dim, int N, int precision, int
                              const int64_t *vmapP, const int64_t *elemtobndy, const double *D,
                              const cb_phys *phys, cb_stream_t stream) {
   if (nghost < 0) return solver_fail(CB_ERR_ARG, "cb_solver_create_ghosted: nghost must be >= 0");
-  if (phys && phys->visc > 0)
-    return solver_fail(CB_ERR_UNSUPPORTED, "cb_solver_create_ghosted: the partitioned form is inviscid");
   return solver_create(out, dim, N, precision, nelem, nghost, Q, rhs, vgeo, sgeo, vmapM, vmapP, elemtobndy, D,
                        phys, stream);
 }
 
-int cb_solver_stage(cb_solver *s, int stage, double dt, void **next_in) {
-  if (!s || stage < 0 || stage > 4) return solver_fail(CB_ERR_ARG, "cb_solver_stage: bad arguments");
+int cb_solver_stage_pass(cb_solver *s, int stage, double dt, int pass, void **next_in) {
+  if (!s || stage < 0 || stage > 4 || pass < 0 || pass > 1)
+    return solver_fail(CB_ERR_ARG, "cb_solver_stage_pass: bad arguments");
   if (!pingpong(s)) return solver_fail(CB_ERR_UNSUPPORTED, "cb_solver_stage: this viscous order has no stage form");
-  const cudaError_t e = s->prec == 64 ? enqueue_one<double>(s, stage, dt) : enqueue_one<float>(s, stage, dt);
+  const cudaError_t e =
+      s->prec == 64 ? enqueue_pass<double>(s, stage, dt, pass) : enqueue_pass<float>(s, stage, dt, pass);
   if (e != cudaSuccess) return solver_fail(CB_ERR_CUDA, "cb_solver_stage: %s", cudaGetErrorString(e));
-  s->cur ^= 1;
+  if (pass == 1) s->cur ^= 1;
   if (next_in) *next_in = s->cur ? s->Qalt : s->Q;
   return CB_OK;
+}
+
+int cb_solver_stage(cb_solver *s, int stage, double dt, void **next_in) {
+  const int rc = cb_solver_stage_pass(s, stage, dt, 0, nullptr);
+  return rc ? rc : cb_solver_stage_pass(s, stage, dt, 1, next_in);
 }
 
 int cb_solver_current(const cb_solver *s, void **state) {
@@ -258,13 +266,14 @@ int cb_solver_settle(cb_solver *s) {
   return e == cudaSuccess ? CB_OK : solver_fail(CB_ERR_CUDA, "cb_solver_settle: %s", cudaGetErrorString(e));
 }
 
-int cb_solver_pack(cb_solver *s, const int64_t *elems, int64_t n, void *buf) {
-  if (!s || n < 0 || (n && (!elems || !buf))) return solver_fail(CB_ERR_ARG, "cb_solver_pack: bad arguments");
+int cb_solver_pack(cb_solver *s, int what, const int64_t *elems, int64_t n, void *buf) {
+  if (!s || n < 0 || (n && (!elems || !buf)) || what < 0 || what > 1 || (what == 1 && !s->gradQ))
+    return solver_fail(CB_ERR_ARG, "cb_solver_pack: bad arguments");
   if (!n) return CB_OK;
   const int Nq = s->N + 1;
-  const int64_t ew = (s->dim == 2 ? (int64_t)Nq * Nq * 4 : (int64_t)Nq * Nq * Nq * 5);
+  const int64_t ew = (s->dim == 2 ? (int64_t)Nq * Nq * 4 : (int64_t)Nq * Nq * Nq * 5) * (what ? s->dim : 1);
   const int grid = (int)std::min<int64_t>((n * ew + 255) / 256, 148 * 16);
-  const void *src = s->cur ? s->Qalt : s->Q;
+  const void *src = what ? s->gradQ : (s->cur ? s->Qalt : s->Q);
   if (s->prec == 64)
     k_pack<double><<<grid, 256, 0, s->stream>>>((const double *)src, elems, n, ew, (double *)buf);
   else
@@ -273,12 +282,14 @@ int cb_solver_pack(cb_solver *s, const int64_t *elems, int64_t n, void *buf) {
   return e == cudaSuccess ? CB_OK : solver_fail(CB_ERR_CUDA, "cb_solver_pack: %s", cudaGetErrorString(e));
 }
 
-int cb_solver_unpack(cb_solver *s, const void *buf, int64_t first, int64_t n) {
-  if (!s || first < 0 || n < 0 || first + n > s->nghost || (n && !buf))
+int cb_solver_unpack(cb_solver *s, int what, const void *buf, int64_t first, int64_t n) {
+  if (!s || what < 0 || what > 1 || (what == 1 && !s->gradQ))
+    return solver_fail(CB_ERR_ARG, "cb_solver_unpack: bad arguments");
+  if (first < 0 || n < 0 || first + n > s->nghost || (n && !buf))
     return solver_fail(CB_ERR_ARG, "cb_solver_unpack: ghost range outside 0..%lld", (long long)s->nghost);
   if (!n) return CB_OK;
-  const size_t ew = state_bytes(s) / (size_t)s->nelem;
-  char *dst = (char *)(s->cur ? s->Qalt : s->Q) + ew * (size_t)(s->nelem + first);
+  const size_t ew = state_bytes(s) / (size_t)s->nelem * (what ? s->dim : 1);
+  char *dst = (char *)(what ? s->gradQ : (s->cur ? s->Qalt : s->Q)) + ew * (size_t)(s->nelem + first);
   const cudaError_t e = cudaMemcpyAsync(dst, buf, ew * (size_t)n, cudaMemcpyDeviceToDevice, s->stream);
   return e == cudaSuccess ? CB_OK : solver_fail(CB_ERR_CUDA, "cb_solver_unpack: %s", cudaGetErrorString(e));
 }
@@ -333,8 +344,12 @@ int solver_create(cb_solver **out, int dim, int N, int precision, int64_t nelem,
   s->part_blocks = 296;
   if ((e = cudaMalloc(&s->part, sizeof(double) * 4 * ns * s->part_blocks)) != cudaSuccess)
     return bail(CB_ERR_NOMEM, "partials");
+  if (phys->visc > 0 && nghost > 0 && !fused_visc(s)) {
+    cb_solver_destroy(s);
+    return solver_fail(CB_ERR_UNSUPPORTED, "cb_solver_create_ghosted: this viscous order has no stage form");
+  }
   if (phys->visc > 0) {
-    const size_t gbytes = w * (size_t)Np * ns * dim * nelem;
+    const size_t gbytes = w * (size_t)Np * ns * dim * (nelem + nghost);
     if ((e = cudaMalloc(&s->gradQ, gbytes)) != cudaSuccess) return bail(CB_ERR_NOMEM, "gradQ");
     cudaMemsetAsync(s->gradQ, 0, gbytes, s->stream);
     if (!fused_visc(s)) {

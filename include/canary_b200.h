@@ -190,16 +190,18 @@ int cb_solver_destroy(cb_solver *s);
  * into contiguous ranges of the Hilbert element order, src/mesh.jl:499-580,
  * with the ghost exchange of its drivers once per RK stage,
  * euler2d_set2c.jl:529-594 / :707-735).  A ghosted solver advances its nelem
- * own elements; Q and the twin hold nghost ghost elements after them, which
- * vmapP may name (elements nelem .. nelem + nghost - 1).  Inviscid form.
- * Before every stage the caller fills the ghost elements of the buffer the
- * stage reads: cb_solver_pack gathers own elements of the current state for
- * a neighbour rank, cb_solver_unpack stores received elements into the
- * current state's ghost range [first, first + n).  cb_solver_stage enqueues
- * one RK stage (0..4) from the current state into the other buffer and
- * returns the new current buffer; cb_solver_settle copies a state left in
- * the twin back into Q (cb_lsrk_run and cb_solver_sums handle it
- * themselves). */
+ * own elements; Q and the twin (and, viscous, the gradient buffer) hold
+ * nghost ghost elements after them, which vmapP may name (elements nelem ..
+ * nelem + nghost - 1).  Before every stage the caller fills the ghosts of the
+ * state the stage reads: cb_solver_pack (what = 0) gathers own elements of
+ * the current state for a neighbour rank, cb_solver_unpack (what = 0) stores
+ * received elements into its ghost range [first, first + n).  The viscous
+ * form (the orders with fused passes) also exchanges the gradient (what = 1)
+ * between the stage's gradient pass and its stage pass
+ * (cb_solver_stage_pass, pass 0 then 1); cb_solver_stage runs both passes.
+ * A stage goes from the current state into the other buffer and returns the
+ * new current buffer; cb_solver_settle copies a state left in the twin back
+ * into Q (cb_lsrk_run and cb_solver_sums handle it themselves). */
 int cb_solver_create_ghosted(cb_solver **out, int dim, int N, int precision,
                              int64_t nelem, int64_t nghost, void *Q, void *rhs,
                              const double *vgeo, const double *sgeo,
@@ -207,10 +209,11 @@ int cb_solver_create_ghosted(cb_solver **out, int dim, int N, int precision,
                              const int64_t *elemtobndy, const double *D,
                              const cb_phys *phys, cb_stream_t stream);
 int cb_solver_stage(cb_solver *s, int stage, double dt, void **next_in);
+int cb_solver_stage_pass(cb_solver *s, int stage, double dt, int pass, void **next_in);
 int cb_solver_current(const cb_solver *s, void **state);
 int cb_solver_settle(cb_solver *s);
-int cb_solver_pack(cb_solver *s, const int64_t *elems, int64_t n, void *buf);
-int cb_solver_unpack(cb_solver *s, const void *buf, int64_t first, int64_t n);
+int cb_solver_pack(cb_solver *s, int what, const int64_t *elems, int64_t n, void *buf);
+int cb_solver_unpack(cb_solver *s, int what, const void *buf, int64_t first, int64_t n);
 
 /* ---------------------------------------------------------------------- */
 /* Device-side geometry.                                                   */

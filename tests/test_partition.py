@@ -37,23 +37,27 @@ def square(N, n):
     return m, Q, 0.002
 
 
-@pytest.mark.parametrize("case,world", [("cube3", 2), ("cube3", 5), ("cube4w", 3), ("square", 4)])
+@pytest.mark.parametrize("case,world,visc", [("cube3", 2, 0.0), ("cube3", 5, 0.0), ("cube4w", 3, 0.0),
+                                             ("square", 4, 0.0), ("cube3", 3, 0.02), ("square", 2, 0.02)])
 @pytest.mark.parametrize("precision", [64, 32])
-def test_parts_equal_single_mesh(case, world, precision):
+def test_parts_equal_single_mesh(case, world, visc, precision):
+    """Inviscid and LDG Navier–Stokes (state and gradient exchanged)."""
     import torch
     m, Q, dt = {"cube3": lambda: cube(3, 4), "cube4w": lambda: cube(4, 3, walls=True),
                 "square": lambda: square(5, 6)}[case]()
     k = 3
-    single = dg.LSRK.for_state(dg.DeviceMesh.upload(m), Q, precision)
+    phys = dict(dg.WORKLOAD_PHYS, visc=visc)
+    single = dg.LSRK.for_state(dg.DeviceMesh.upload(m), Q, precision, phys=dg.make_phys(**phys))
     single.run(k, dt)
     ref = single.state()
     single.close()
     stream = torch.cuda.Stream()
-    parts = [P.GhostedLSRK(m, P.plan(m, r, world), Q, precision, stream=stream) for r in range(world)]
+    parts = [P.GhostedLSRK(m, P.plan(m, r, world), Q, precision, dg.make_phys(**phys), stream=stream)
+             for r in range(world)]
     P.run_parts(parts, k, dt)
     got = np.concatenate([p.state() for p in parts], axis=2)
     for p in parts:
         p.close()
     assert np.array_equal(got, ref)
     if precision == 64:
-        assert max(relerr_fields(got, oracle_run(m, Q, dt, k))) < 1e-12
+        assert max(relerr_fields(got, oracle_run(m, Q, dt, k, phys=phys))) < 1e-12

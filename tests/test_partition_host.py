@@ -42,14 +42,14 @@ class _Rows:
 
     def __init__(self, p, ew=3):
         import torch
-        self.p, self.ew = p, ew
+        self.p, self.ew, self.widths = p, ew, (ew, ew)
         self.Q = torch.full((p.nloc + p.nghost, ew), -1.0, dtype=torch.float64)
         self.Q[:p.nloc] = torch.arange(p.lo, p.hi, dtype=torch.float64)[:, None] * 10 + torch.arange(ew)
 
-    def pack(self, idx, buf):
+    def pack(self, idx, buf, what=0):
         buf.copy_(self.Q[idx].reshape(-1))
 
-    def unpack(self, buf, first, n):
+    def unpack(self, buf, first, n, what=0):
         i = self.p.nloc + first
         self.Q[i:i + n] = buf.reshape(n, self.ew)
 
