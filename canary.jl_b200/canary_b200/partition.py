@@ -115,7 +115,8 @@ class GhostedLSRK:
         ns, Np = nstate(mesh.dim), mesh.Np
         self.ew = ns * Np
         self.visc = self.phys.visc > 0
-        self.widths = (self.ew, self.ew * mesh.dim)  # element width of the state and of its gradient
+        # element width of the state and of its gradient (viscous form only)
+        self.widths = (self.ew, self.ew * mesh.dim if self.visc else self.ew)
         Q = np.asarray(Q, dtype=np.float64)
         if offset is None:
             offset = Q.mean(axis=(0, 2)) if precision == 32 else np.zeros(ns)
