@@ -7,6 +7,7 @@
 module CanaryB200
 
 using CUDA  # CuArray, CuPtr, CUDA.stream()
+using MPI   # lowstorageRK_mpi
 
 const libcb = joinpath(@__DIR__, "..", "lib", "libcanary_b200.so")
 
@@ -65,6 +66,60 @@ function lowstorageRK(::Val{dim}, ::Val{N}, d_QL::CuArray{Float64}, d_rhsL, d_vg
                 d_elemtobndy, d_D, phys, stream()))
     try
         check(ccall((:cb_lsrk_run, libcb), Cint, (Ptr{Cvoid}, Int64, Float64), h[], nsteps, dt))
+    finally
+        ccall((:cb_solver_destroy, libcb), Cint, (Ptr{Cvoid},), h[])
+    end
+    nothing
+end
+
+# Element-partitioned lowstorageRK over MPI ranks, with the reference's
+# partition and ghost bookkeeping (connectmesh, src/mesh.jl:751-956:
+# realelems then ghostelems, sendelems, nabrtorank / nabrtorecv /
+# nabrtosend) and its exchange of whole elements before every stage
+# (euler2d_set2c.jl:529-594, :707-735), through the ghosted solver's stage API.
+# d_QL holds the real elements followed by the ghost elements; the MPI
+# library must accept device buffers.
+function lowstorageRK_mpi(::Val{dim}, ::Val{N}, mpicomm, d_QL::CuArray{Float64}, d_rhsL, d_vgeoL,
+                          d_sgeo, d_vmapM, d_vmapP, d_elemtobndy, d_D, nrealelem, sendelems,
+                          nabrtorank, nabrtorecv, nabrtosend, dt, nsteps;
+                          phys = REFERENCE_PHYS) where {dim, N}
+    nghost = size(d_QL, ndims(d_QL)) - nrealelem
+    ew = length(d_QL) ÷ size(d_QL, ndims(d_QL))  # values per element
+    h = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((:cb_solver_create_ghosted, libcb), Cint,
+                (Ref{Ptr{Cvoid}}, Cint, Cint, Cint, Int64, Int64, CuPtr{Float64}, CuPtr{Float64},
+                 CuPtr{Float64}, CuPtr{Float64}, CuPtr{Int64}, CuPtr{Int64}, CuPtr{Int64},
+                 CuPtr{Float64}, Ref{CbPhys}, Ptr{Cvoid}),
+                h, dim, N, 64, nrealelem, nghost, d_QL, d_rhsL, d_vgeoL, d_sgeo, d_vmapM, d_vmapP,
+                d_elemtobndy, d_D, phys, stream()))
+    sendidx = [CuArray{Int64}(sendelems[r] .- 1) for r in nabrtosend]  # 0-based own elements
+    sendbuf = [CuArray{Float64}(undef, ew * length(r)) for r in nabrtosend]
+    recvbuf = [CuArray{Float64}(undef, ew * length(r)) for r in nabrtorecv]
+    next = Ref{Ptr{Cvoid}}(C_NULL)
+    try
+        for step in 1:nsteps, s in 0:4
+            for n in eachindex(nabrtorank)
+                check(ccall((:cb_solver_pack, libcb), Cint,
+                            (Ptr{Cvoid}, Cint, CuPtr{Int64}, Int64, CuPtr{Float64}),
+                            h[], 0, sendidx[n], length(sendidx[n]), sendbuf[n]))
+            end
+            CUDA.synchronize()
+            reqs = MPI.Request[]
+            for n in eachindex(nabrtorank)
+                push!(reqs, MPI.Irecv!(recvbuf[n], nabrtorank[n], 777, mpicomm))
+                push!(reqs, MPI.Isend(sendbuf[n], nabrtorank[n], 777, mpicomm))
+            end
+            MPI.Waitall!(reqs)
+            for n in eachindex(nabrtorank)
+                check(ccall((:cb_solver_unpack, libcb), Cint,
+                            (Ptr{Cvoid}, Cint, CuPtr{Float64}, Int64, Int64),
+                            h[], 0, recvbuf[n], first(nabrtorecv[n]) - nrealelem - 1,
+                            length(nabrtorecv[n])))
+            end
+            check(ccall((:cb_solver_stage, libcb), Cint, (Ptr{Cvoid}, Cint, Float64, Ref{Ptr{Cvoid}}),
+                        h[], s, dt, next))
+        end
+        check(ccall((:cb_solver_settle, libcb), Cint, (Ptr{Cvoid},), h[]))
     finally
         ccall((:cb_solver_destroy, libcb), Cint, (Ptr{Cvoid},), h[])
     end
