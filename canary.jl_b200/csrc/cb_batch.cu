@@ -297,6 +297,7 @@ struct cb_batch {
   std::vector<BSlot> slots;
   int64_t steps = 0;  // batch steps launched (the device counter after them)
   int var[2][BMAXN2 + 1] = {};
+  int64_t last_used[NSHAPE] = {};  // batch step at which each shape last had live instances
   bool affine = true;  // use the affine-element stage where it applies
   // one step as a graph; re-built when the set of shapes present changes
   cudaGraphExec_t exec = nullptr;
@@ -460,11 +461,18 @@ int batch_run(cb_batch *b, int64_t nsteps) {
     }
   const int64_t launch = std::min(need, nsteps);
   if (launch <= 0) return CB_OK;
-  // keep the shapes of the current graph: a shape whose instances have all
-  // left costs a few empty launches per step, while re-building the graph
-  // each time a shape comes and goes (continuous batching) costs milliseconds
-  shapes |= b->g_shapes;
-  if (!b->exec || shapes != b->g_shapes) {
+  // Under continuous batching shapes come and go; re-building the graph
+  // costs milliseconds, an empty shape a few empty launches per step.  So a
+  // graph keeps the shapes used in the last KEEP_STEPS steps: it is re-built
+  // when a new shape appears or when a shape has been idle that long.
+  constexpr int64_t KEEP_STEPS = 256;
+  for (int sid = 0; sid < NSHAPE; ++sid)
+    if (shapes.test(sid)) b->last_used[sid] = b->steps;
+  std::bitset<NSHAPE> keep = shapes;
+  for (int sid = 0; sid < NSHAPE; ++sid)
+    if (b->g_shapes.test(sid) && b->steps - b->last_used[sid] < KEEP_STEPS) keep.set(sid);
+  if (!b->exec || (shapes & ~b->g_shapes).any() || keep != b->g_shapes) {
+    shapes = keep;
     drop_graph(b);
     cudaError_t e = build_graph<T>(b, shapes);
     if (e != cudaSuccess) {
