@@ -86,3 +86,31 @@ def test_batch_argument_validation_without_device():
     assert L.cb_batch_release(None, 0) == _lib.CB_ERR_ARG
     assert L.cb_batch_info(None, 0, None, None) == _lib.CB_ERR_ARG
     assert L.cb_batch_destroy(None) == _lib.CB_OK and L.cb_mesh_destroy(None) == _lib.CB_OK
+
+
+def test_partition_and_setup_argument_validation_without_device():
+    """The stage / exchange API of the partitioned solve and the device brick
+    mesh reject bad arguments before touching the device."""
+    L = _lib.lib()
+    phys = _lib.cb_phys(1.4, 1.0, 3.5, 2.5, 0.0, 0.72, -2 / 3, 0.0)
+    dummy = C.c_void_p(16)
+    h = C.c_void_p()
+    nxt = C.c_void_p()
+    assert L.cb_solver_create_ghosted(C.byref(h), 3, 3, 64, 8, -1, dummy, dummy, dummy, dummy, dummy, dummy,
+                                      dummy, dummy, C.byref(phys), None) == _lib.CB_ERR_ARG
+    assert L.cb_solver_stage(None, 0, 1e-3, C.byref(nxt)) == _lib.CB_ERR_ARG
+    assert L.cb_solver_stage_pass(None, 0, 1e-3, 0, C.byref(nxt)) == _lib.CB_ERR_ARG
+    assert L.cb_solver_settle(None) == _lib.CB_ERR_ARG
+    assert L.cb_solver_current(None, C.byref(nxt)) == _lib.CB_ERR_ARG
+    assert L.cb_solver_pack(None, 0, dummy, 1, dummy) == _lib.CB_ERR_ARG
+    assert L.cb_solver_unpack(None, 0, dummy, 0, 1) == _lib.CB_ERR_ARG
+    n = (C.c_int64 * 3)(2, 2, 2)
+    xs = (C.c_void_p * 3)(16, 16, 16)
+    per = (C.c_int * 3)(1, 1, 1)
+    assert L.cb_brickmesh(4, 3, n, xs, per, None, dummy, dummy, dummy, dummy, None) == _lib.CB_ERR_ARG
+    bad = (C.c_int64 * 3)(2, 0, 2)
+    assert L.cb_brickmesh(3, 3, bad, xs, per, None, dummy, dummy, dummy, dummy, None) == _lib.CB_ERR_ARG
+    assert L.cb_mesh_affine(None, None) == _lib.CB_ERR_ARG
+    assert L.cb_batch_set_affine(None, 1) == _lib.CB_ERR_ARG
+    assert L.cb_batch_slot_variant(None, 0, None) == _lib.CB_ERR_ARG
+
