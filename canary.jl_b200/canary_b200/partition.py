@@ -102,14 +102,15 @@ def plan(mesh: Mesh, rank: int, world: int) -> PartPlan:
 
 class GhostedLSRK:
     """A rank's solver (cb_solver_create_ghosted) for its part of `mesh`,
-    starting from the global host state Q (Np, nstate, nelem).  All work is
-    ordered on `stream` (a torch stream; the current one by default)."""
+    starting from the global host state Q (Np, nstate, nelem).  All its work
+    — stages, packing, unpacking — is ordered on `stream` (a torch stream; a
+    new one by default), on which the exchange of its buffers must run too."""
 
     def __init__(self, mesh: Mesh, p: PartPlan, Q: np.ndarray, precision=64, phys=None, stream=None,
                  device="cuda", offset=None):
         torch = _torch()
         self.mesh, self.plan, self.precision = mesh, p, precision
-        self.stream = stream or torch.cuda.current_stream(torch.device(device))
+        self.stream = stream or torch.cuda.Stream(torch.device(device))
         self.real = torch.float64 if precision == 64 else torch.float32
         self.phys = phys or make_phys()
         ns, Np = nstate(mesh.dim), mesh.Np
@@ -249,8 +250,10 @@ class PartitionedLSRK:
 def run_parts(parts, nsteps: int, dt: float) -> None:
     """Advance several parts of one mesh held by this process (one GPU) in
     lock step, moving ghosts by device copies: the partitioned arithmetic
-    without the inter-rank transport."""
+    without the inter-rank transport.  The parts must share one stream."""
     torch = _torch()
+    if any(p.stream != parts[0].stream for p in parts):
+        raise ValueError("run_parts: the parts must be created on one stream")
     bufs = {}
     for r, part in enumerate(parts):
         for q, first, n in part.plan.recv:
