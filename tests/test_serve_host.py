@@ -37,3 +37,23 @@ def test_plan_reaches_the_final_time():
     r3 = S.Request(1, "euler3d", 7, 16, 0.5, 0.0)
     n3, dt3 = S.plan(r3, 1.3)
     assert n3 == math.ceil(0.5 / (0.2 * (2 * math.pi / 16) / (49 * 1.3)))
+
+
+def test_mesh_pool_evicts_idle_meshes_least_recently_used_first():
+    class _BM:
+        closed = 0
+
+        def close(self):
+            _BM.closed += 1
+
+    pool = S.MeshPool(device=None, stream=None)
+    for k, (nbytes, users, last) in {"a": (40, 0, 3.0), "b": (30, 1, 1.0), "c": (20, 0, 2.0)}.items():
+        pool.meshes[k] = S._Mesh(None, nbytes, {32: _BM()}, users, last)
+    assert pool.resident_bytes() == 90
+    assert pool.evict(need=5, budget=100, in_use=0)          # fits: nothing evicted
+    assert set(pool.meshes) == {"a", "b", "c"}
+    assert pool.evict(need=25, budget=100, in_use=0)         # drops "c" (idle, oldest idle)
+    assert set(pool.meshes) == {"a", "b"} and _BM.closed == 1
+    assert not pool.evict(need=80, budget=100, in_use=0)     # "b" is in use: cannot make room
+    assert set(pool.meshes) == {"b"} and _BM.closed == 2
+    assert S.MeshPool.nbytes(3, 3, 4, 32) > S.MeshPool.nbytes(3, 3, 4, 64) > 0
