@@ -172,10 +172,10 @@ def setup_device_workload(n_side, N, precision, device="cuda", seed=0):
     return dm, Q, torch.zeros_like(Q), dt, off
 
 
-def cpu_sample(N, seconds=10.0, n_side=16, max_steps=40):
-    """Oracle (CPU restatement of the reference's CPU path) on a bounded
-    sample of the workload: same N, warp and initial-state law on an
-    n_side^3 mesh, all host threads, LSRK steps until `seconds` elapse."""
+def _oracle_rate(N, seconds, n_side, max_steps, cores):
+    """DOF·stage/s of the oracle on an n_side^3 sample of the workload with
+    `cores` OpenMP threads, LSRK steps until `seconds` elapse; (rate, steps,
+    seconds)."""
     from canary_b200 import dg
     from oracle import pyoracle as O
     mesh, Q, dt = setup_workload(n_side, N, device=None)
@@ -183,7 +183,6 @@ def cpu_sample(N, seconds=10.0, n_side=16, max_steps=40):
     wp["lambda"] = wp.pop("lam")
     phys = O.make_phys(**wp)
     rhs = np.zeros_like(Q, order="F")
-    cores = os.cpu_count() or 1
     O.lowstorageRK(3, N, mesh.vgeo, mesh.sgeo, Q, rhs, mesh.D, dt, 1, mesh.vmapM, mesh.vmapP,
                    mesh.elemtobndy, phys, cores)  # warm-up
     t0 = time.perf_counter()
@@ -193,10 +192,23 @@ def cpu_sample(N, seconds=10.0, n_side=16, max_steps=40):
                        mesh.elemtobndy, phys, cores)
         steps += 1
     el = time.perf_counter() - t0
-    dof = mesh.nelem * mesh.Np * 5
-    return {"value": dof * 5 * steps / el, "unit": METRIC, "cores": cores, "kind": "port",
+    return mesh.nelem * mesh.Np * 5 * 5 * steps / el, steps, el
+
+
+def cpu_sample(N, seconds=10.0, n_side=16, max_steps=40):
+    """Oracle (CPU restatement of the reference's CPU path) on a bounded
+    sample of the workload: same N, warp and initial-state law on an
+    n_side^3 mesh, all host threads, LSRK steps until `seconds` elapse; and,
+    mirroring the reference's single-threaded Julia loop, one thread on an
+    8^3 sample."""
+    cores = os.cpu_count() or 1
+    rate, steps, el = _oracle_rate(N, seconds, n_side, max_steps, cores)
+    r1, s1, e1 = _oracle_rate(N, seconds / 2, 8, 4, 1)
+    return {"value": rate, "unit": METRIC, "cores": cores, "kind": "port",
             "sample": f"{n_side}^3 hexes N={N} (same warp/IC law), {steps} LSRK steps "
-                      f"({5 * steps} stages) in {el:.1f} s, C oracle with {cores} OpenMP threads"}
+                      f"({5 * steps} stages) in {el:.1f} s, C oracle with {cores} OpenMP threads",
+            "single_thread": {"value": r1, "unit": METRIC, "cores": 1,
+                              "sample": f"8^3 hexes N={N}, {s1} LSRK steps in {e1:.1f} s, one thread"}}
 
 
 def batched_ensemble(count=512, seed=0, steps=500, device="cuda"):
