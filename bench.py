@@ -15,7 +15,19 @@ Under torchrun each rank advances its own copy of the workload (independent
 replicas, "weak" scaling); the timed region is bracketed by a barrier and a
 device synchronisation and the slowest rank's time is reported.
 `--impl reference` times the CPU restatement of the reference's CPU path on
-the host cores instead (rank 0 only).
+the host cores instead (rank 0 only), on the same workload.
+
+After the timed region (one GPU) the line also carries:
+  * e2e: the same steps through the public API with the state uploaded from
+    and read back to pinned host memory every step;
+  * parity.config1: the timed workload advanced by 200 steps on the GPU and
+    by the oracle from the same device-built mesh and state (bar 1e-12); the
+    oracle's timing on all host cores is the cpu_baseline;
+  * precision_form: FP32 against FP64 at 32^3, N = 4, 7, 10, 1000 steps, the
+    LDG Navier-Stokes variant and the 2-D vortex (bar 1e-5);
+  * batched: 512 vortex instances in one batch per precision, with a roofline
+    and 16 instances checked against the oracle;
+  * served: the served request stream.
 """
 from __future__ import annotations
 
@@ -211,12 +223,134 @@ def cpu_sample(N, seconds=10.0, n_side=16, max_steps=40):
                               "sample": f"8^3 hexes N={N}, {s1} LSRK steps in {e1:.1f} s, one thread"}}
 
 
-def batched_ensemble(count=512, seed=0, steps=500, device="cuda"):
+def _oracle_phys():
+    from canary_b200 import dg
+    from oracle import pyoracle as O
+    wp = dict(dg.WORKLOAD_PHYS)
+    wp["lambda"] = wp.pop("lam")
+    return O.make_phys(**wp)
+
+
+def _rel_l2(a, b):
+    """Relative L2 error per state field (axis 1 of (Np, nstate, nelem))."""
+    return [float(np.linalg.norm(a[:, q] - b[:, q]) / np.linalg.norm(b[:, q])) for q in range(b.shape[1])]
+
+
+class Config1Parity:
+    """Full-size parity of the bench workload: the FP64 GPU solver and the
+    oracle (the CPU restatement of the reference's lowstorageRK,
+    euler3d_set3c.jl:1361-1523) each advance the same initial state on the
+    same mesh (the device-built geometry and maps, copied to the host) by the
+    stated step count; the relative L2 error per field is compared with 1e-12.
+    The oracle runs on all host cores in a background thread (ctypes releases
+    the GIL), so the GPU sections that follow overlap it; its timing over the
+    whole workload is the CPU baseline."""
+
+    NAMES = ("U", "V", "W", "rho", "E")
+
+    def __init__(self, dm, Q0, dt, steps, stream, threads):
+        import torch
+        from canary_b200 import dg
+        m = dm.mesh
+        Nfp = (m.N + 1) ** 2
+        self.steps, self.threads, self.dt = steps, threads, dt
+        shape = (m.Np, 5, m.nelem)
+        q = Q0.clone()
+        r = torch.zeros_like(q)
+        s = dg.LSRK(dm, q, r, 64, dg.make_phys(), stream)
+        s.run(steps, dt)
+        torch.cuda.synchronize()
+        self.gpu = dg.from_device(q, shape)
+        s.close()
+        del q, r
+        self.m = m
+        self.vgeo = dg.from_device(dm.vgeo, (m.Np, 14, m.nelem))
+        self.sgeo = dg.from_device(dm.sgeo, (5, Nfp, 6, m.nelem))
+        self.vmapM = dg.from_device(dm.vmapM, (Nfp, 6, m.nelem))
+        self.vmapP = dg.from_device(dm.vmapP, (Nfp, 6, m.nelem))
+        self.etb = dg.from_device(dm.elemtobndy, (6, m.nelem))
+        self.Q = np.asfortranarray(dg.from_device(Q0, shape))
+        self.out = None
+        self.thread = threading.Thread(target=self._oracle, daemon=True)
+        self.thread.start()
+
+    def _oracle(self):
+        from oracle import pyoracle as O
+        rhs = np.zeros_like(self.Q, order="F")
+        t0 = time.perf_counter()
+        O.lowstorageRK(3, self.m.N, self.vgeo, self.sgeo, self.Q, rhs, self.m.D, self.dt, self.steps,
+                       self.vmapM, self.vmapP, self.etb, _oracle_phys(), self.threads)
+        self.seconds = time.perf_counter() - t0
+
+    def result(self):
+        self.thread.join()
+        err = _rel_l2(self.gpu, self.Q)
+        dof = self.m.nelem * self.m.Np * 5
+        return {
+            "workload": "the bench workload (32^3 hexes, N=7, warped, seeded Fourier state) as timed, "
+                        "device-built mesh and state copied to the oracle",
+            "steps": self.steps, "dt": self.dt, "bar": 1e-12,
+            "rel_l2": dict(zip(self.NAMES, err)), "max_rel_l2": max(err), "pass": max(err) <= 1e-12,
+            "finite": bool(np.all(np.isfinite(self.gpu))),
+            "oracle_seconds": self.seconds, "oracle_threads": self.threads,
+            "oracle_value": dof * 5 * self.steps / self.seconds,
+        }
+
+
+def precision_section(steps=1000, orders=(4, 7, 10), n_side=32, ns_n_side=16, device="cuda"):
+    """The precision form at full size: FP32 against the FP64 form (itself
+    pinned to the oracle) after `steps` steps on the same mesh and initial
+    state, inviscid 3-D at n_side^3, the LDG Navier-Stokes variant
+    (mu = 1e-3, Pr = 0.72) at ns_n_side^3 and the 2-D vortex."""
+    from canary_b200 import precision as P
+    cases = []
+    for c in P.report(orders, n_side, steps, ns_n_side, device=device):
+        cases.append({"dim": c["dim"], "N": c["N"], "n_side": c["n_side"], "visc": c["visc"], "steps": steps,
+                      "dt": c["dt"], "rel_l2": c["fp32_rel_l2_vs_fp64"], "max_rel_l2": c["max_rel_l2"],
+                      "fp64_dof_stage_per_s": c["fp64"]["dof_stage_per_s"],
+                      "fp32_dof_stage_per_s": c["fp32"]["dof_stage_per_s"],
+                      "fp32_mass_drift_rel": c["fp32"]["mass_drift_rel"],
+                      "finite": c["fp64"]["finite"] and c["fp32"]["finite"]})
+    worst = max(c["max_rel_l2"] for c in cases)
+    return {"workload": f"warped [0,2π]^3 {n_side}^3 (LDG NS {ns_n_side}^3) and 2-D vortex 10^2, FP32 vs FP64, "
+                        f"dt = min(CFL rule, 0.08/steps)",
+            "bar": 1e-5, "max_rel_l2": worst, "pass": worst <= 1e-5, "cases": cases}
+
+
+def ensemble_parity(params, cache, finals, sample=16, steps=500, dt=0.002, threads=None):
+    """The first `sample` instances of the batched ensemble through the
+    oracle (FP64, `steps` steps from the same host mesh and initial state)
+    against the FP64 batch (bar 1e-12) and the FP32 batch (bar 1e-5)."""
+    from canary_b200 import batch as B
+    from oracle import pyoracle as O
+    threads = threads or os.cpu_count() or 1
+    e64 = np.zeros(4)
+    e32 = np.zeros(4)
+    t0 = time.perf_counter()
+    for i, p in enumerate(params[:sample]):
+        m = cache.host(2, p["N"], p["n_side"])
+        Q = B.vortex_state(m, p["beta"], p["xc"], p["yc"])
+        rhs = np.zeros_like(Q, order="F")
+        O.lowstorageRK(2, p["N"], m.vgeo, m.sgeo, Q, rhs, m.D, dt, steps, m.vmapM, m.vmapP, m.elemtobndy,
+                       _oracle_phys(), threads)
+        e64 = np.maximum(e64, _rel_l2(finals[64][i], Q))
+        e32 = np.maximum(e32, _rel_l2(finals[32][i], Q))
+    names = ("U", "V", "rho", "E")
+    return {"instances": min(sample, len(params)), "steps": steps,
+            "shapes": [(p["N"], p["n_side"]) for p in params[:sample]],
+            "fp64_vs_oracle": dict(zip(names, e64.tolist())), "fp64_bar": 1e-12,
+            "fp32_vs_oracle": dict(zip(names, e32.tolist())), "fp32_bar": 1e-5,
+            "pass": bool(e64.max() <= 1e-12 and e32.max() <= 1e-5),
+            "oracle_seconds": time.perf_counter() - t0}
+
+
+def batched_ensemble(count=512, seed=0, steps=500, device="cuda", parity_sample=16):
     """The batched workload: `count` independent 2-D vortex instances (N, mesh,
     strength and centre drawn per instance from PCG64(seed + i)), dt = 0.002,
     `steps` LSRK(5,4) steps each, advanced together by one Batch per precision
-    (one graph launch per step).  Returns throughput, solves/s and the FP32
-    form's relative L2 error per field against the FP64 batch."""
+    (one graph launch per step).  Returns throughput, solves/s, the roofline
+    of the step, the FP32 form's relative L2 error per field against the FP64
+    batch and a sample of instances checked against the oracle."""
     import torch
     from canary_b200 import batch as B, ic
     params = ic.vortex_ensemble(count, seed)
@@ -245,18 +379,41 @@ def batched_ensemble(count=512, seed=0, steps=500, device="cuda"):
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
         st = ens.batch.status()
+        # algorithmic HBM bytes of one step: per instance nodes x bytes per
+        # node and stage of the stage variant it runs (the affine-element
+        # stage reads one geometry record per element instead of the
+        # per-node metric and face geometry)
+        w = 8 if prec == 64 else 4
+        step_bytes = 0.0
+        for p, slot in zip(params, ens.slots):
+            Np = (p["N"] + 1) ** 2
+            nodes = Np * p["n_side"] ** 2
+            if ens.batch.slot_variant(slot) == B.VAR_AFFINE:
+                bpn = w * (4 * 4 + 17.0 / Np)  # state + carry, record of 17 values per element
+            else:
+                bpn = bytes_per_node(2, p["N"], w)
+            step_bytes += 5 * nodes * bpn
+        peak, peak_kind = measured_peaks()
+        achieved = step_bytes / (ms * 1e-3 / (steps - 1)) / 1e9
         finals[prec] = ens.results()
         out[f"fp{prec}"] = {"value": ens.dof * 5 * (steps - 1) / (ms * 1e-3), "unit": METRIC,
                             "ms_per_step": ms / (steps - 1), "dof": ens.dof,
                             "solves_per_s": count / (ms * 1e-3 * steps / (steps - 1)),
                             "state_finite": not bool(st.any()),
-                            "variants": {f"{d},{n}": v for (d, n), v in ens.variants().items()}}
+                            "variants": {f"{d},{n}": v for (d, n), v in ens.variants().items()},
+                            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                                         "frac": achieved / peak, "peak_kind": peak_kind,
+                                         "bytes_per_step": step_bytes,
+                                         "kernel": "k_stage_pipe2 (one persistent kernel per shape, "
+                                                   "five stage launches per step)"}}
         ens.close()
     err = np.zeros(4)
     for a, b in zip(finals[32], finals[64]):
         for q in range(4):
             err[q] = max(err[q], np.linalg.norm(a[:, q] - b[:, q]) / np.linalg.norm(b[:, q]))
     out["fp32_rel_l2_vs_fp64_max_over_instances"] = {"U": err[0], "V": err[1], "rho": err[2], "E": err[3]}
+    if parity_sample:
+        out["parity_vs_oracle"] = ensemble_parity(params, cache, finals, parity_sample, steps)
     cache.close()
     return out
 
@@ -276,19 +433,34 @@ def dist_init():
     return rank, ws, local, tdist
 
 
+def reference_workload(n_side, N, seed=0):
+    """The bench workload built for the CPU path alone: the oracle's
+    restatement of the reference's set-up (brickmesh -> partition ->
+    connectmesh -> mappings -> computegeometry with the sinusoidal warp) and
+    the seeded Fourier state (257 modes, evaluated by torch: on a GPU where
+    one is present, else on the host cores; set-up only, never timed)."""
+    import torch
+    from canary_b200 import ic
+    from oracle import pyoracle as O
+    L = 2 * math.pi
+    S = O.setup(3, N, (np.linspace(0.0, L, n_side + 1),) * 3, (True,) * 3, warp=1, warp_amp=0.05)
+    X = [np.ascontiguousarray(S.vgeo[:, 11 + c, :]) for c in range(3)]
+    f = ic.fourier_state(*X, seed=seed, device="cuda" if torch.cuda.is_available() else "cpu")
+    Q = np.asfortranarray(np.stack(f, axis=1))
+    dt = ic.fourier_dt(Q, N, h=L / n_side)
+    return S, Q, dt
+
+
 def run_reference(args, rank):
-    """--impl reference: the CPU path on the host cores (rank 0 only)."""
+    """--impl reference: the CPU path on the host cores (rank 0 only), on the
+    same workload as the GPU arm."""
     if rank != 0:
         return
-    from canary_b200 import dg
     from oracle import pyoracle as O
-    pyoracle_build = O.build
-    pyoracle_build()
-    n_side = args.ref_n_side
-    mesh, Q, dt = setup_workload(n_side, args.order, device=None)
-    wp = dict(dg.WORKLOAD_PHYS)
-    wp["lambda"] = wp.pop("lam")
-    phys = O.make_phys(**wp)
+    O.build()
+    n_side = args.ref_n_side or args.n_side
+    mesh, Q, dt = reference_workload(n_side, args.order)
+    phys = _oracle_phys()
     rhs = np.zeros_like(Q, order="F")
     cores = os.cpu_count() or 1
     for _ in range(args.warmup):
@@ -299,20 +471,21 @@ def run_reference(args, rank):
         O.lowstorageRK(3, args.order, mesh.vgeo, mesh.sgeo, Q, rhs, mesh.D, dt, 1, mesh.vmapM,
                        mesh.vmapP, mesh.elemtobndy, phys, cores)
     el = time.perf_counter() - t0
-    dof = mesh.nelem * mesh.Np * 5
+    dof = mesh.nelem * (args.order + 1) ** 3 * 5
     val = dof * 5 * args.steps / el
     line = {
         "impl": "reference", "metric": METRIC, "value": val, "unit": METRIC,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"3-D Euler, periodic [0,2π]^3 warped, N={args.order}, "
-                               f"bounded CPU sample {n_side}^3 hexes of the {args.n_side}^3 workload",
-                   "n_side": n_side, "order": args.order, "dt": dt},
+        "config": {"workload": f"3-D Euler, periodic [0,2π]^3, {n_side}^3 hexes, N={args.order}, "
+                               "warped x_i += 0.05 sin x sin y sin z, seeded Fourier state (seed 0)",
+                   "n_side": n_side, "order": args.order, "nelem": mesh.nelem, "dof": dof, "dt": dt,
+                   "same_config": n_side == args.n_side},
         "cpu_baseline": {"value": val, "unit": METRIC, "cores": cores, "kind": "port",
-                         "sample": f"{n_side}^3 hexes, N={args.order}, {args.steps} timed LSRK steps; "
-                                   "the reference's Julia CPU path cannot run here (no Julia toolchain), "
-                                   "so its C restatement (oracle/) is timed"},
+                         "sample": f"{n_side}^3 hexes, N={args.order}, {args.steps} timed LSRK steps "
+                                   f"after {args.warmup} untimed; the reference's Julia CPU path cannot run "
+                                   "here (no Julia toolchain), so its C restatement (oracle/) is timed"},
         "e2e": {"value": val, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -327,8 +500,13 @@ def main():
     ap.add_argument("--precision", type=int, default=64, choices=[64, 32])
     ap.add_argument("--n-side", type=int, default=32)
     ap.add_argument("--order", type=int, default=7)
-    ap.add_argument("--ref-n-side", type=int, default=8)
-    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--ref-n-side", type=int, default=None,
+                    help="mesh of the reference arm (default: --n-side, the same workload)")
+    ap.add_argument("--e2e-steps", type=int, default=8)
+    ap.add_argument("--parity-steps", type=int, default=200,
+                    help="steps of the full-size parity run against the oracle (0: skip)")
+    ap.add_argument("--precision-steps", type=int, default=1000,
+                    help="steps of the precision-form section (0: skip)")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true",
@@ -360,6 +538,7 @@ def main():
     solver = dg.LSRK(dm, dQ, drhs, args.precision, dg.make_phys(), stream)
     solver.set_offset(off)
     dof = mesh.nelem * mesh.Np * 5
+    dQ0 = dQ.clone()  # initial state, for the parity run
 
     solver.run(args.warmup, dt)
     torch.cuda.synchronize(dev)
@@ -389,23 +568,58 @@ def main():
     # end to end through the public API with host buffers: every step copies
     # the state from pinned host memory, advances one step and reads the
     # state back (the step's input is the state alone: the 2N-storage carry
-    # is zero at a step boundary, scaled by RKA[0] = 0 after the fifth stage)
+    # is zero at a step boundary, scaled by RKA[0] = 0 after the fifth stage).
+    # Two device states, each with its own solver on the compute stream, and
+    # one copy stream per direction: the upload of step k+1 and the read-back
+    # of step k overlap step k's compute and each other.
     hQ = torch.empty(dQ.numel(), dtype=real, pin_memory=True)
     hQ.copy_(dQ)
-    hout = torch.empty_like(hQ, pin_memory=True)
+    hout = [torch.empty_like(hQ, pin_memory=True) for _ in range(2)]
+    dQ2 = [dQ, torch.empty_like(dQ)]
+    rhs2 = [drhs, torch.zeros_like(drhs)]
+    solvers = [solver, dg.LSRK(dm, dQ2[1], rhs2[1], args.precision, dg.make_phys(), stream)]
+    solvers[1].set_offset(off)
+    up, down = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
     torch.cuda.synchronize(dev)
     if tdist is not None:
         tdist.barrier()
+    ev = lambda: torch.cuda.Event(enable_timing=False)
+    loaded, stepped, stored = [], [], []
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    f0.record(stream)
-    for _ in range(args.e2e_steps):
-        dQ.copy_(hQ, non_blocking=True)
-        solver.run(1, dt)
-        hout.copy_(dQ, non_blocking=True)
-    f1.record(stream)
+    f0.record(up)
+    for k in range(args.e2e_steps):
+        b = k % 2
+        if k >= 2:
+            up.wait_event(stored[k - 2])  # state buffer b has been read back
+        with torch.cuda.stream(up):
+            dQ2[b].copy_(hQ, non_blocking=True)
+        loaded.append(ev())
+        loaded[k].record(up)
+        stream.wait_event(loaded[k])
+        solvers[b].run(1, dt)
+        stepped.append(ev())
+        stepped[k].record(stream)
+        down.wait_event(stepped[k])
+        with torch.cuda.stream(down):
+            hout[b].copy_(dQ2[b], non_blocking=True)
+        stored.append(ev())
+        stored[k].record(down)
+    f1.record(down)
     torch.cuda.synchronize(dev)
     e2e_ms = replicas.max_over_ranks(f0.elapsed_time(f1), device=dev)
-    solver.close()
+    e2e_ok = bool(torch.equal(hout[(args.e2e_steps - 1) % 2], hout[(args.e2e_steps - 2) % 2]))
+    for sv in solvers:
+        sv.close()
+    del dQ2, rhs2, hout
+
+    # full-size parity of the timed workload (FP64 form): the oracle runs on
+    # the host cores in the background while the precision section uses the GPU
+    par = None
+    if rank == 0 and world == 1 and args.precision == 64 and args.parity_steps > 0:
+        par = Config1Parity(dm, dQ0, dt, args.parity_steps, stream, os.cpu_count() or 1)
+    prec_sec = None
+    if world == 1 and args.precision_steps > 0:
+        prec_sec = precision_section(args.precision_steps, device=dev)
 
     w = 8 if args.precision == 64 else 4
     bpn = bytes_per_node(dim, N, w)
@@ -435,14 +649,31 @@ def main():
                      "traffic": traffic, "bytes_per_node": bpn, "kernel": "k_stage_pipe2",
                      "launch_ms": t_launch * 1e3},
         "e2e": {"value": world * dof * 5 * args.e2e_steps / (e2e_ms * 1e-3), "unit": METRIC,
-                "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo, "steps": args.e2e_steps},
+                "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo, "steps": args.e2e_steps,
+                "ms_per_step": e2e_ms / args.e2e_steps, "results_repeat": e2e_ok,
+                "how": "cb_solver per state buffer; H2D, step and D2H on three streams, two states in flight"},
         "gpu_launches": launches,
         "clocks": clk,
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if prec_sec is not None:
+        line["precision_form"] = prec_sec
+    if par is not None:
+        res = par.result()
+        line["parity"] = {"config1": res}
+        if not args.no_cpu_baseline:
+            r1, s1, e1 = _oracle_rate(N, args.cpu_seconds / 2, 8, 4, 1)
+            line["cpu_baseline"] = {
+                "value": res["oracle_value"], "unit": METRIC, "cores": res["oracle_threads"], "kind": "port",
+                "sample": f"the whole timed workload ({args.n_side}^3 hexes, N={N}), all {args.parity_steps} "
+                          f"steps of the parity run in {res['oracle_seconds']:.1f} s, C oracle with "
+                          f"{res['oracle_threads']} OpenMP threads (overlapping GPU work of this process)",
+                "single_thread": {"value": r1, "unit": METRIC, "cores": 1,
+                                  "sample": f"8^3 hexes N={N}, {s1} LSRK steps in {e1:.1f} s, one thread"}}
+    elif rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_sample(N, args.cpu_seconds)
     if world == 1 and not args.no_batched:
-        bat = batched_ensemble(args.batched_instances, device=dev)
+        bat = batched_ensemble(args.batched_instances, device=dev,
+                               parity_sample=16 if args.parity_steps > 0 else 0)
         if args.precision == 64:
             bat["fp32_over_fp64_plain"] = bat["fp32"]["value"] / value
         line["batched"] = bat

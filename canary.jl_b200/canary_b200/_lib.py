@@ -24,7 +24,8 @@ EXPORTS = (
     "cb_updatesolution", "cb_updatesolution_f32",
     "cb_volume_grad", "cb_flux_grad", "cb_update_gradQ", "cb_volume_div", "cb_flux_div",
     "cb_solver_create", "cb_lsrk_run", "cb_solver_set_offset", "cb_solver_sums",
-    "cb_solver_destroy", "cb_solver_status_async", "cb_lsrk_stage_noalloc",
+    "cb_solver_destroy", "cb_solver_status_async", "cb_lsrk_stage_noalloc", "cb_noalloc_status",
+    "cb_solver_reset_status", "cb_solver_test_timeout",
     "cb_solver_create_ghosted", "cb_solver_stage", "cb_solver_stage_pass", "cb_solver_current", "cb_solver_settle",
     "cb_solver_pack", "cb_solver_unpack",
     "cb_computegeometry", "cb_brickmesh", "cb_mesh_create", "cb_mesh_affine", "cb_mesh_destroy",
@@ -93,6 +94,7 @@ def lib() -> C.CDLL:
     L.cb_solver_unpack.argtypes = [vp, C.c_int, vp, i64, i64]
     L.cb_lsrk_stage_noalloc.argtypes = [C.c_int, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp, i64,
                                         phys_p, dbl, dbl, dbl, vp, vp]
+    L.cb_noalloc_status.argtypes = [vp, C.POINTER(C.c_uint)]
     L.cb_computegeometry.argtypes = [C.c_int, C.c_int, i64, vp, dbl, vp, vp, vp, vp, vp, vp]
     L.cb_mesh_create.argtypes = [C.POINTER(vp), C.c_int, C.c_int, C.c_int, i64, vp, vp, vp, vp, vp, vp, vp]
     L.cb_mesh_destroy.argtypes = [vp]
@@ -111,6 +113,8 @@ def lib() -> C.CDLL:
     L.cb_batch_destroy.argtypes = [vp]
     L.cb_batch_status_async.argtypes = [vp, vp]
     L.cb_solver_status_async.argtypes = [vp, vp]
+    L.cb_solver_reset_status.argtypes = [vp]
+    L.cb_solver_test_timeout.argtypes = [vp]
     _lib = L
     return L
 

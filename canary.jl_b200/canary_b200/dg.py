@@ -196,7 +196,8 @@ def lsrk_stage_noalloc(dim, N, Q, rhs, vgeo, sgeo, vmapM, vmapP, elemtobndy, D, 
     that own every device allocation): same result as volumerhs, fluxrhs and
     updatesolution in sequence.  Its scratch is a fixed static device array
     shared by all calls, so calls must not overlap on the GPU.  `status`, if
-    given, is a CUDA int32 tensor that receives the kernel status bits."""
+    given, is a CUDA int32 tensor that receives the kernel status bits;
+    otherwise they go to a sticky word that `noalloc_status` reads."""
     torch = _torch()
     n = _nelem(elems)
     Np, Nfp, nf = _sizes(dim, N, n)
@@ -207,6 +208,15 @@ def lsrk_stage_noalloc(dim, N, Q, rhs, vgeo, sgeo, vmapM, vmapP, elemtobndy, D, 
         _ptr(vmapP, torch.int64), _ptr(elemtobndy, torch.int64), _ptr(D, torch.float64), n,
         C.byref(phys or make_phys()), float(rka), float(rkb), float(dt),
         _ptr(status, torch.int32) if status is not None else None, _stream(stream)))
+
+
+def noalloc_status(stream=None) -> int:
+    """Synchronise, read and clear the sticky status word of the
+    allocation-free stage (calls made with status=None); raises CanaryError
+    for a set bit, else returns 0."""
+    bits = C.c_uint(0)
+    check(_lib.lib().cb_noalloc_status(_stream(stream), C.byref(bits)))
+    return bits.value
 
 
 def device_status(stream=None) -> None:
@@ -425,6 +435,17 @@ class LSRK:
         """Enqueue a copy of the status bits into `host` (a pinned int32
         tensor) on the solver's stream."""
         check(_lib.lib().cb_solver_status_async(self._h, C.c_void_p(host.data_ptr())))
+
+    def reset_status(self) -> None:
+        """Clear the solver's sticky status bits (stream-ordered)."""
+        check(_lib.lib().cb_solver_reset_status(self._h))
+
+    def test_timeout(self) -> None:
+        """Test hook of the bounded device waits: enqueue one stage whose
+        first state copy per block is withheld, so that every block's wait
+        gives up; the stage stores nothing and raises the timeout status
+        (CB_ERR_TIMEOUT from `sums`)."""
+        check(_lib.lib().cb_solver_test_timeout(self._h))
 
     def sums(self) -> np.ndarray:
         """Compensated FP64 (Σ MJ Q_s, Σ MJ Q_s²) per field, shape (2, nstate)."""

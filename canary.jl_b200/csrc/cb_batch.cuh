@@ -702,6 +702,8 @@ struct BatchSrc {
     wpos = wpos < 0 ? -1 : publish_from(wpos + gridDim.x, ring[(it + RING - 1) % RING]);
     if (wpos < 0 && (threadIdx.x & 31) == 0) ring[(it + RING - 1) % RING].valid = 0;
   }
+  __device__ bool skip_copy(int) const { return false; }
+  __device__ uint32_t wait_limit() const { return WAIT_LIMIT; }
   __device__ const BItem<T> &at(int it) const { return ring[it % RING]; }
   __device__ bool valid(int it) const { return at(it).valid != 0; }
   __device__ bool last(int it) const { return at(it).last != 0; }

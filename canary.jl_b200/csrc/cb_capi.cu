@@ -189,6 +189,7 @@ int cb_device_status(cb_stream_t stream) {
   if (h & ST_BC) return fail(CB_ERR_BC, "invalid boundary condition code (only 0 and 1 are defined)");
   if (h & ST_MESH) return fail(CB_ERR_MESH, "vmapP points outside the mesh (those faces were skipped)");
   if (h & ST_NONFINITE) return fail(CB_ERR_NONFINITE, "non-finite state");
+  if (h & ST_TIMEOUT) return fail(CB_ERR_TIMEOUT, "a bounded device wait gave up (that stage stored nothing)");
   return CB_OK;
 }
 

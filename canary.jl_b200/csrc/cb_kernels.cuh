@@ -795,10 +795,12 @@ struct Launch {
                                                                 vmapP, bnd, p, status);
     return cudaGetLastError();
   }
+  // probe != 0: the timeout test hook of the pipelined stage (see MeshSrc);
+  // shapes without that stage return cudaErrorNotSupported for it.
   static cudaError_t stage(const T *Qin, T *Qout, T *rhs, const T *vgeo, const T *sgeo,
                            const int32_t *nbr, const T *D, int64_t nelem, const PhysT<T> &p,
                            const Offs<T, NS> &qref, T rka, T rkbdt, unsigned *status,
-                           cudaStream_t st) {
+                           cudaStream_t st, int probe = 0) {
     constexpr bool pipe_ok = Pipe<DIM, Nq, T>::OK;
     const bool aligned = ((reinterpret_cast<uintptr_t>(Qin) | reinterpret_cast<uintptr_t>(vgeo)) & 15) == 0;
     const bool aligned2 = aligned && ((reinterpret_cast<uintptr_t>(rhs) | reinterpret_cast<uintptr_t>(sgeo)) & 15) == 0;
@@ -806,20 +808,28 @@ struct Launch {
       using PP = Pipe2<DIM, Nq, T>;
       using S = MeshSrc<T, NS, C::EPB>;
       const size_t sm = PP::smem();
-      static int per_sm = 0;  // resident blocks per SM, from the occupancy calculator
-      if (!per_sm) {
-        cudaError_t err = prep(k_stage_pipe2<DIM, Nq, T, S>, sm);
+      // resident blocks per SM, from the occupancy calculator, per device
+      static int per_sm[MAX_DEVICES] = {0};
+      int dev = 0;
+      cudaError_t err = cudaGetDevice(&dev);
+      if (err != cudaSuccess) return err;
+      if (dev < 0 || dev >= MAX_DEVICES) return cudaErrorInvalidDevice;
+      if (!per_sm[dev]) {
+        err = prep(k_stage_pipe2<DIM, Nq, T, S>, sm);
         if (err != cudaSuccess) return err;
-        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stage_pipe2<DIM, Nq, T, S>, C::THREADS, sm);
+        int v = 0;
+        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_stage_pipe2<DIM, Nq, T, S>, C::THREADS, sm);
         if (err != cudaSuccess) return err;
-        if (per_sm < 1) per_sm = 1;
+        per_sm[dev] = v < 1 ? 1 : v;
       }
       const int64_t groups = (nelem + C::EPB - 1) / C::EPB;
-      int64_t g = (int64_t)num_sms() * per_sm;
+      int64_t g = (int64_t)num_sms() * per_sm[dev];
       if (g > groups) g = groups;
-      const S src{Qin, Qout, rhs, vgeo, sgeo, nbr, D, nelem, qref, rkbdt, status};
+      const S src{Qin, Qout, rhs, vgeo, sgeo, nbr, D, nelem, qref, rkbdt, status, probe};
       k_stage_pipe2<DIM, Nq, T, S><<<(int)g, C::THREADS, sm, st>>>(src, p, rka);
       return cudaGetLastError();
+    } else if (probe) {
+      return cudaErrorNotSupported;
     } else if (pipe_ok && aligned) {
       using PP = Pipe<DIM, Nq, T>;
       size_t sm = PP::smem();

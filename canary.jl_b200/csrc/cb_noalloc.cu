@@ -8,8 +8,9 @@
 // as cb_volumerhs + cb_fluxrhs + cb_updatesolution (visc = 0) in one fused
 // pass, with all of its scratch — the copy of the stage's input state that
 // neighbour traces are read from, the compact face-neighbour table and a
-// status word — in a fixed file-scope device array instead of memory from
-// cudaMalloc.
+// sticky status word — in a fixed file-scope device array instead of memory
+// from cudaMalloc.  cb_noalloc_status reads (and clears) the sticky word
+// without allocating either.
 #include <cuda_runtime.h>
 
 #include <cstdarg>
@@ -32,26 +33,36 @@ constexpr size_t ALIGN = 256;
 // Every GPU that loads the library holds this array until the process exits.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[SCRATCH_BYTES];
 
+constexpr int MAX_DEVICES = 128;  // devices whose scratch address is cached
 std::mutex g_mu;
-void *g_addr[128] = {nullptr};
+void *g_addr[MAX_DEVICES] = {nullptr};
 
 size_t up(size_t b) { return (b + ALIGN - 1) / ALIGN * ALIGN; }
 
+// Scratch layout: [sticky status word | face-neighbour table | stage-input state].
+// The status word is never cleared by a stage call (the array starts zeroed
+// when the library's device code is loaded); cb_noalloc_status clears it.
+constexpr size_t OFF_NBR = ALIGN;
+
 // Device address of the scratch array for the current device.  In host code
 // the array's name is only a host-side stand-in, so the address is looked up
-// once per device, with that device current.
-int scratch_address(void **out) {
+// once per device, with that device current, and kept for the life of the
+// process: after cudaDeviceReset (or any reset of the primary context) the
+// cached address is stale, so a process that resets a device must not call
+// the allocation-free entry points again.
+int scratch_address(void **out, const char *who) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess || dev < 0 || dev >= 128)
-    return solver_fail(CB_ERR_CUDA, "cb_lsrk_stage_noalloc: cudaGetDevice: %s", cudaGetErrorString(e));
+  if (e != cudaSuccess) return solver_fail(CB_ERR_CUDA, "%s: cudaGetDevice: %s", who, cudaGetErrorString(e));
+  if (dev < 0 || dev >= MAX_DEVICES)
+    return solver_fail(CB_ERR_UNSUPPORTED, "%s: device %d is beyond the %d devices this library tracks", who, dev,
+                       MAX_DEVICES);
   std::lock_guard<std::mutex> lk(g_mu);
   if (!g_addr[dev]) {
     void *p = nullptr;
     e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || !p)
-      return solver_fail(CB_ERR_CUDA, "cb_lsrk_stage_noalloc: cudaGetSymbolAddress: %s",
-                         cudaGetErrorString(e));
+      return solver_fail(CB_ERR_CUDA, "%s: cudaGetSymbolAddress: %s", who, cudaGetErrorString(e));
     g_addr[dev] = p;
   }
   *out = g_addr[dev];
@@ -73,26 +84,30 @@ extern "C" int cb_lsrk_stage_noalloc(int dim, int N, double *Q, double *rhs, con
   if (!o) return solver_fail(CB_ERR_UNSUPPORTED, "cb_lsrk_stage_noalloc: order N=%d outside 1..%d", N, MAXN);
   if (nelem == 0) return CB_OK;
   const int ns = dim == 2 ? 4 : 5, nface = 2 * dim;
-  const size_t qbytes = sizeof(double) * (size_t)o->Np * ns * (size_t)nelem;
-  const size_t nbytes = sizeof(int32_t) * (size_t)nface * (size_t)nelem;
-  const size_t need = up(sizeof(unsigned)) + up(nbytes) + up(qbytes);
-  if (need > SCRATCH_BYTES)
+  // reject before any size arithmetic can wrap: the neighbour table and the
+  // state copy together take this many bytes per element, plus two padded
+  // boundaries
+  const size_t per_elem = sizeof(double) * (size_t)o->Np * ns + sizeof(int32_t) * (size_t)nface;
+  const size_t max_elems = (SCRATCH_BYTES - OFF_NBR - 2 * ALIGN) / per_elem;
+  const size_t qbytes = (size_t)nelem <= max_elems ? sizeof(double) * (size_t)o->Np * ns * (size_t)nelem : 0;
+  const size_t nbytes = sizeof(int32_t) * (size_t)nface * ((size_t)nelem <= max_elems ? (size_t)nelem : 0);
+  const size_t need = OFF_NBR + up(nbytes) + up(qbytes);
+  if ((size_t)nelem > max_elems || need > SCRATCH_BYTES)
     return solver_fail(CB_ERR_ARG,
-                       "cb_lsrk_stage_noalloc: nelem=%lld at dim=%d, N=%d needs %zu bytes of scratch; "
-                       "the static scratch holds %zu bytes (use cb_solver_create for larger meshes)",
-                       (long long)nelem, dim, N, need, SCRATCH_BYTES);
+                       "cb_lsrk_stage_noalloc: nelem=%lld at dim=%d, N=%d exceeds the %zu elements that "
+                       "the static scratch of %zu bytes holds (use cb_solver_create for larger meshes)",
+                       (long long)nelem, dim, N, max_elems, SCRATCH_BYTES);
   void *base = nullptr;
-  int rc = scratch_address(&base);
+  int rc = scratch_address(&base, "cb_lsrk_stage_noalloc");
   if (rc) return rc;
   unsigned char *b = (unsigned char *)base;
-  unsigned *own_status = (unsigned *)b;
-  int32_t *nbr = (int32_t *)(b + up(sizeof(unsigned)));
-  double *Qin = (double *)(b + up(sizeof(unsigned)) + up(nbytes));
-  unsigned *st = status ? status : own_status;
+  unsigned *sticky = (unsigned *)b;
+  int32_t *nbr = (int32_t *)(b + OFF_NBR);
+  double *Qin = (double *)(b + OFF_NBR + up(nbytes));
+  unsigned *st = status ? status : sticky;
   cudaStream_t s = (cudaStream_t)stream;
   cudaError_t e;
-  if ((e = cudaMemsetAsync(own_status, 0, sizeof(unsigned), s)) != cudaSuccess ||
-      (e = o->prepare()) != cudaSuccess ||
+  if ((e = o->prepare()) != cudaSuccess ||
       (e = o->build_nbr(nbr, vmapM, vmapP, elemtobndy, nelem, st, s)) != cudaSuccess ||
       (e = cudaMemcpyAsync(Qin, Q, qbytes, cudaMemcpyDeviceToDevice, s)) != cudaSuccess)
     return solver_fail(CB_ERR_CUDA, "cb_lsrk_stage_noalloc: %s", cudaGetErrorString(e));
@@ -102,5 +117,23 @@ extern "C" int cb_lsrk_stage_noalloc(int dim, int N, double *Q, double *rhs, con
                              phys->lambda, phys->visc});
   e = o->stage(Qin, Q, rhs, vgeo, sgeo, nbr, D, nelem, p, q0, rka, rkb * dt, st, s);
   if (e != cudaSuccess) return solver_fail(CB_ERR_CUDA, "cb_lsrk_stage_noalloc: %s", cudaGetErrorString(e));
+  return CB_OK;
+}
+
+extern "C" int cb_noalloc_status(cb_stream_t stream, unsigned *bits) {
+  void *base = nullptr;
+  int rc = scratch_address(&base, "cb_noalloc_status");
+  if (rc) return rc;
+  unsigned h = 0;
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e;
+  if ((e = cudaMemcpyAsync(&h, base, sizeof h, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+      (e = cudaMemsetAsync(base, 0, sizeof h, s)) != cudaSuccess || (e = cudaStreamSynchronize(s)) != cudaSuccess)
+    return solver_fail(CB_ERR_CUDA, "cb_noalloc_status: %s", cudaGetErrorString(e));
+  if (bits) *bits = h;
+  if (h & ST_BC) return solver_fail(CB_ERR_BC, "invalid boundary condition code (only 0 and 1 are defined)");
+  if (h & ST_MESH) return solver_fail(CB_ERR_MESH, "vmapM/vmapP do not describe a conforming mesh");
+  if (h & ST_NONFINITE) return solver_fail(CB_ERR_NONFINITE, "non-finite state");
+  if (h & ST_TIMEOUT) return solver_fail(CB_ERR_TIMEOUT, "a bounded device wait gave up");
   return CB_OK;
 }

@@ -68,11 +68,18 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
+// Devices for which per-device launch facts (SM count, occupancy) are cached.
+constexpr int MAX_DEVICES = 128;
+
 inline int num_sms() {
-  static int cached[64] = {0};
+  static int cached[MAX_DEVICES] = {0};
   int dev = 0;
   cudaGetDevice(&dev);
-  if (dev < 0 || dev >= 64) dev = 0;
+  if (dev < 0 || dev >= MAX_DEVICES) {
+    int v = 0;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+    return v > 0 ? v : 148;
+  }
   if (!cached[dev]) {
     int v = 0;
     cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
@@ -82,6 +89,8 @@ inline int num_sms() {
 }
 
 constexpr uint32_t WAIT_LIMIT = 1u << 22;
+// Poll limit of the timeout test hook (a wait that is meant to give up).
+constexpr uint32_t PROBE_WAIT_LIMIT = 1u << 12;
 constexpr size_t SMEM_LIMIT = 227 * 1024;
 
 // Row stride (in elements) of the contraction buffers: >= Nq, a multiple of
@@ -294,7 +303,7 @@ k_stage_pipe(const T *__restrict__ Qin, T *__restrict__ Qout, T *__restrict__ rh
     }
 
     // ---- wait for this group's slabs (each thread observes the mbarrier; a
-    // wait that gives up flags the status word and the iteration continues)
+    // wait that gives up is agreed on at the mid-iteration barrier)
     if constexpr (PP::BULK) {
       if (!mbar_wait_bounded(&bars[b], (uint32_t)((it >> 1) & 1), WAIT_LIMIT)) timed_out = true;
     } else {
@@ -375,7 +384,19 @@ k_stage_pipe(const T *__restrict__ Qin, T *__restrict__ Qout, T *__restrict__ rh
         for (int s = 0; s < NS; ++s) FF[(f * NS + s) * FS + el * Nfp + fn] = smj[u] * out[s];
       }
     }
-    __syncthreads();
+    // A wait that gave up: store nothing for this group, flag the status,
+    // let the issued copies land (bounded) and leave.
+    if (__syncthreads_or(timed_out)) {
+      if (tid == 0) {
+        atomicOr(status, ST_TIMEOUT);
+        if constexpr (PP::BULK) {
+          mbar_wait_bounded(&bars[b], (uint32_t)((it >> 1) & 1), WAIT_LIMIT);
+          if (gn < ngroups) mbar_wait_bounded(&bars[b ^ 1], (uint32_t)(((it + 1) >> 1) & 1), WAIT_LIMIT);
+        }
+      }
+      if constexpr (!PP::BULK) cp_async_wait<0>();
+      return;
+    }
     // ---- phase B: carry - source + volume contraction - face terms, update
 #pragma unroll
     for (int u = 0; u < C::NPT; ++u) {
@@ -400,7 +421,6 @@ k_stage_pipe(const T *__restrict__ Qin, T *__restrict__ Qout, T *__restrict__ rh
   }
   if constexpr (!PP::BULK) cp_async_wait<0>();
   if (bad) atomicOr(status, ST_NONFINITE);
-  if (timed_out) atomicOr(status, ST_TIMEOUT);
 }
 
 }  // namespace cb

@@ -111,6 +111,12 @@ struct MeshSrc {
   Offs<T, NS> qref_;
   T rkbdt_;
   unsigned *status_;
+  // Test hook (0 in every production launch): the state copy of each block's
+  // first group is never issued and waits give up after PROBE_WAIT_LIMIT
+  // polls, so that the bounded wait runs out on an mbarrier nobody arrives on.
+  int probe_;
+  __device__ bool skip_copy(int it) const { return probe_ != 0 && it == 0; }
+  __device__ uint32_t wait_limit() const { return probe_ ? PROBE_WAIT_LIMIT : WAIT_LIMIT; }
   __device__ void begin(unsigned char *) {}
   __device__ void prefetch() {}
   __device__ void publish(int) {}
@@ -183,6 +189,7 @@ k_stage_pipe2(Src src, PhysT<T> p, T rka) {
       *reinterpret_cast<T *>(reinterpret_cast<unsigned char *>(dst) + b) = *reinterpret_cast<const T *>(base + b);
   };
   auto issue_S = [&](int it, int b) {  // thread 0 only
+    if (src.skip_copy(it)) return;
     const int64_t e0 = src.e0(it);
     const int nv = src.nv(it);
     const bool last = PP::RAG && src.last(it);
@@ -292,8 +299,8 @@ k_stage_pipe2(Src src, PhysT<T> p, T rka) {
     }
 
     // ---- wait for S[sb] (state + metric) and T[tb] (carry + sgeo)
-    if (!mbar_wait_bounded(&barS[sb], (uint32_t)((it / PP::NSB) & 1), WAIT_LIMIT)) timed_out = true;
-    if (!mbar_wait_bounded(&barT[tb], (uint32_t)((it / PP::NTB) & 1), WAIT_LIMIT)) timed_out = true;
+    if (!mbar_wait_bounded(&barS[sb], (uint32_t)((it / PP::NSB) & 1), src.wait_limit())) timed_out = true;
+    if (!mbar_wait_bounded(&barT[tb], (uint32_t)((it / PP::NTB) & 1), src.wait_limit())) timed_out = true;
     // staged slabs (RAG: each source's data starts `head` bytes into its slab)
     const T *Sq = S0 + sb * SSTRIDE + head_of(Qin + e0 * Np * NS) / sizeof(T);
     const T *Sg = S0 + sb * SSTRIDE + PP::QBS / sizeof(T);
@@ -410,7 +417,24 @@ k_stage_pipe2(Src src, PhysT<T> p, T rka) {
         for (int s = 0; s < NS; ++s) FF[(f * NS + s) * FS + el * Nfp + fn] = smj * out[s];
       }
     }
-    __syncthreads();
+    // The mid-iteration barrier also agrees on whether any thread's wait gave
+    // up.  If one did, the block stores nothing for this group (its slabs may
+    // be incomplete), flags the status word, lets the copies it has issued
+    // land (bounded waits, so a copy that never completes cannot hold the
+    // block) and leaves: later groups of this block are not computed either.
+    if (__syncthreads_or(timed_out)) {
+      if (tid == 0) {
+        atomicOr(src.status(it), ST_TIMEOUT);
+        // in flight: S of groups it .. it + LOOK - 1 (the copy of it + LOOK
+        // is issued after this barrier), T of groups it .. it + LOOK; each
+        // barrier holds at most one pending phase, the group's parity
+        for (int g = it; g < it + PP::LOOK && src.valid(g); ++g)
+          mbar_wait_bounded(&barS[g % PP::NSB], (uint32_t)((g / PP::NSB) & 1), src.wait_limit());
+        for (int g = it; g <= it + PP::LOOK && src.valid(g); ++g)
+          mbar_wait_bounded(&barT[g % PP::NTB], (uint32_t)((g / PP::NTB) & 1), src.wait_limit());
+      }
+      return;
+    }
     // S[sb] is no longer read: refill it while phase B runs
     if (tid == 0 && more) issue_S(it + PP::LOOK, sb);
     if ((tid >> 5) == (Src::PUBLISHER >> 5)) src.publish(it);
@@ -441,10 +465,6 @@ k_stage_pipe2(Src src, PhysT<T> p, T rka) {
       }
     }
     if (bad) atomicOr(src.status(it), ST_NONFINITE);
-    if (timed_out) {
-      atomicOr(src.status(it), ST_TIMEOUT);
-      timed_out = false;
-    }
     __syncthreads();  // T[tb], the flux rows, FF and the item ring are free for reuse
   }
 }

@@ -467,6 +467,8 @@ int cb_solver_sums(cb_solver *s, double *out_host) {
     // q = 2*s + k  (k = 0: Σ MJ Q, k = 1: Σ MJ Q²) -> out[k*ns + s]
     out_host[(q % 2) * ns + q / 2] = sum + comp;
   }
+  if (st & ST_TIMEOUT)
+    return solver_fail(CB_ERR_TIMEOUT, "a bounded device wait gave up: a stage stored nothing, the state is stale");
   if (st & ST_NONFINITE) return solver_fail(CB_ERR_NONFINITE, "the state became non-finite");
   if (st & ST_BC) return solver_fail(CB_ERR_BC, "invalid boundary condition code");
   return CB_OK;
@@ -483,6 +485,40 @@ int cb_solver_set_offset(cb_solver *s, const double *qref) {
   for (int k = 0; k < (s->dim == 2 ? 4 : 5); ++k) s->qref[k] = qref[k];
   drop_graph(s);
   return CB_OK;
+}
+
+int cb_solver_reset_status(cb_solver *s) {
+  if (!s) return solver_fail(CB_ERR_ARG, "cb_solver_reset_status: null solver");
+  const cudaError_t e = cudaMemsetAsync(s->status, 0, sizeof(unsigned), s->stream);
+  return e == cudaSuccess ? CB_OK : solver_fail(CB_ERR_CUDA, "cb_solver_reset_status: %s", cudaGetErrorString(e));
+}
+
+int cb_solver_test_timeout(cb_solver *s) {
+  if (!s) return solver_fail(CB_ERR_ARG, "cb_solver_test_timeout: null solver");
+  if (s->phys.visc > 0)
+    return solver_fail(CB_ERR_UNSUPPORTED, "cb_solver_test_timeout: the inviscid pipelined stage only");
+  const PhysT<double> p64(Phys{s->phys.gamma, s->phys.R_gas, s->phys.c_p, s->phys.c_v, s->phys.gravity, s->phys.Pr,
+                               s->phys.lambda, s->phys.visc});
+  const PhysT<float> p32(Phys{s->phys.gamma, s->phys.R_gas, s->phys.c_p, s->phys.c_v, s->phys.gravity, s->phys.Pr,
+                              s->phys.lambda, s->phys.visc});
+  void *a = s->cur ? s->Qalt : s->Q, *b = s->cur ? s->Q : s->Qalt;
+  cudaError_t e;
+  if (s->prec == 64) {
+    Offs<double, 5> q5;
+    for (int k = 0; k < 5; ++k) q5.v[k] = s->qref[k];
+    e = ops<double>(s)->stage_probe((const double *)a, (double *)b, (double *)s->rhs, (const double *)s->vgeo,
+                                    (const double *)s->sgeo, s->nbr, (const double *)s->D, s->nelem, p64, q5,
+                                    RKA[1], RKB[0], s->status, s->stream);
+  } else {
+    Offs<float, 5> q5;
+    for (int k = 0; k < 5; ++k) q5.v[k] = (float)s->qref[k];
+    e = ops<float>(s)->stage_probe((const float *)a, (float *)b, (float *)s->rhs, (const float *)s->vgeo,
+                                   (const float *)s->sgeo, s->nbr, (const float *)s->D, s->nelem, p32, q5,
+                                   (float)RKA[1], (float)RKB[0], s->status, s->stream);
+  }
+  if (e == cudaErrorNotSupported)  // returned by the launcher, not by CUDA
+    return solver_fail(CB_ERR_UNSUPPORTED, "cb_solver_test_timeout: this shape does not run the pipelined stage");
+  return e == cudaSuccess ? CB_OK : solver_fail(CB_ERR_CUDA, "cb_solver_test_timeout: %s", cudaGetErrorString(e));
 }
 
 int cb_solver_status_async(cb_solver *s, unsigned *out_host) {

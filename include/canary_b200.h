@@ -184,6 +184,16 @@ int cb_solver_sums(cb_solver *s, double *out_host);
  * non-finite state) into *out_host (page-locked memory for an asynchronous
  * copy); the value is valid once the stream has reached the copy. */
 int cb_solver_status_async(cb_solver *s, unsigned *out_host);
+/* Clear the solver's sticky status bits (stream-ordered). */
+int cb_solver_reset_status(cb_solver *s);
+/* Test hook of the bounded waits (no counterpart in the reference): enqueue
+ * one inviscid stage of the pipelined kernel in which each block's first
+ * state copy is never issued and the mbarrier waits give up after a short
+ * poll limit.  Every block then stores nothing, sets status bit 8
+ * (reported as CB_ERR_TIMEOUT by cb_solver_sums), lets its issued copies
+ * land and exits; the state and the residual carry are left unchanged.
+ * CB_ERR_UNSUPPORTED for shapes that do not run the pipelined stage. */
+int cb_solver_test_timeout(cb_solver *s);
 int cb_solver_destroy(cb_solver *s);
 
 /* Element-partitioned solve (one rank per GPU, the reference's partition
@@ -366,8 +376,11 @@ int cb_batch_destroy(cb_batch *b);
  * Every call shares the one array, so calls that overlap on the GPU (other
  * streams, other host threads) race; serialise them.  Kernel-detected
  * problems (boundary code other than 0/1, vmaps that are not a conforming
- * mesh, non-finite state) are OR-ed into *status when status is a non-NULL
- * device pointer (the caller clears it). */
+ * mesh, non-finite state, a bounded wait that gave up) are OR-ed into *status
+ * when status is a non-NULL device pointer (the caller clears it), and into a
+ * sticky word inside the static array when status is NULL.  The address of
+ * the array is looked up once per device and kept: a process that resets a
+ * device (cudaDeviceReset) must not call these entry points afterwards. */
 int cb_lsrk_stage_noalloc(int dim, int N, double *Q, double *rhs,
                           const double *vgeo, const double *sgeo,
                           const int64_t *vmapM, const int64_t *vmapP,
@@ -375,6 +388,12 @@ int cb_lsrk_stage_noalloc(int dim, int N, double *Q, double *rhs,
                           int64_t nelem, const cb_phys *phys, double rka,
                           double rkb, double dt, unsigned *status,
                           cb_stream_t stream);
+/* Reads and clears, on the current device, the sticky status word that
+ * cb_lsrk_stage_noalloc calls with status == NULL raise; synchronises
+ * `stream`.  Writes the raw bits to *bits (if non-NULL) and returns
+ * CB_ERR_BC, CB_ERR_MESH, CB_ERR_NONFINITE, CB_ERR_TIMEOUT or CB_OK.
+ * Allocates nothing. */
+int cb_noalloc_status(cb_stream_t stream, unsigned *bits);
 
 #ifdef __cplusplus
 }

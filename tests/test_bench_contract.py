@@ -8,7 +8,10 @@ import sys
 
 def test_reference_arm_prints_the_contract_line():
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-    out = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--steps", "1", "--warmup", "0"],
+    # by default the arm runs the GPU arm's own workload (--n-side); a small
+    # one here keeps the CPU suite fast
+    out = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--steps", "1", "--warmup", "0",
+                          "--n-side", "6"],
                          cwd=root, capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stderr[-2000:]
     line = json.loads(out.stdout.strip().splitlines()[-1])
@@ -16,5 +19,7 @@ def test_reference_arm_prints_the_contract_line():
               "scaling", "vs_baseline", "dtype", "data", "config", "impl", "cpu_baseline", "e2e"):
         assert k in line, k
     assert line["impl"] == "reference" and line["value"] > 0
+    assert line["config"]["same_config"] and line["config"]["n_side"] == 6
+    assert line["config"]["dof"] == 6 ** 3 * 8 ** 3 * 5
     assert line["cpu_baseline"]["value"] == line["value"] and line["cpu_baseline"]["cores"] >= 1
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0

@@ -28,14 +28,42 @@ def _relerr(a, b):
     return max(out)
 
 
+def _max_elements(dim, N):
+    """Largest element count the 32 MiB static scratch accepts: a sticky status
+    word padded to 256 bytes, then the int32 face-neighbour table and the FP64
+    stage-input state, each padded to 256 bytes."""
+    Np, ns, nface = (N + 1) ** dim, 5 if dim == 3 else 4, 2 * dim
+    return (dg.NOALLOC_SCRATCH_BYTES - 256 - 2 * 256) // (8 * Np * ns + 4 * nface)
+
+
 def test_noalloc_rejects_meshes_beyond_the_static_scratch():
     phys = cb_phys(1.4, 1.0, 3.5, 2.5, 0.0, 0.72, -2 / 3, 0.0)
     import ctypes as C
     d = C.c_void_p(16)  # never dereferenced: the size check comes first
-    rc = lib().cb_lsrk_stage_noalloc(3, 7, d, d, d, d, d, d, d, d, 10 ** 6, C.byref(phys),
-                                     0.0, 0.1, 0.1, None, None)
+    for n in (10 ** 6, 2 ** 62):  # the second would wrap a naive byte count
+        rc = lib().cb_lsrk_stage_noalloc(3, 7, d, d, d, d, d, d, d, d, n, C.byref(phys),
+                                         0.0, 0.1, 0.1, None, None)
+        assert rc == CB_ERR_ARG
+        assert "scratch" in lib().cb_last_error().decode()
+
+
+@pytest.mark.skipif(cuda_available(), reason="passes fake pointers past the size check: CPU only")
+@pytest.mark.parametrize("dim,N", [(3, 7), (2, 4), (3, 1)])
+def test_noalloc_size_boundary(dim, N):
+    """One element above the limit is rejected before any device work; the
+    limit itself passes the size check (without a GPU the call then fails
+    at the device lookup, never with CB_ERR_ARG)."""
+    import ctypes as C
+    phys = cb_phys(1.4, 1.0, 3.5, 2.5, 0.0, 0.72, -2 / 3, 0.0)
+    d = C.c_void_p(16)
+    n = _max_elements(dim, N)
+    rc = lib().cb_lsrk_stage_noalloc(dim, N, d, d, d, d, d, d, d, d, n + 1, C.byref(phys), 0.0, 0.1, 0.1,
+                                     None, None)
     assert rc == CB_ERR_ARG
-    assert "scratch" in lib().cb_last_error().decode()
+    assert f"exceeds the {n} elements" in lib().cb_last_error().decode()
+    rc = lib().cb_lsrk_stage_noalloc(dim, N, d, d, d, d, d, d, d, d, n, C.byref(phys), 0.0, 0.1, 0.1,
+                                     None, None)
+    assert rc != CB_ERR_ARG
 
 
 @pytest.mark.gpu
@@ -78,3 +106,37 @@ def test_noalloc_stage_matches_stateless_entry_points(dim, N, n):
         assert _relerr(qb_h, qa_h) < 1e-13, call
         assert _relerr(rb_h, ra_h) < 1e-11, call
     assert int(status.item()) == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not cuda_available(), reason="needs a CUDA GPU")
+def test_noalloc_reports_kernel_status_with_and_without_a_status_word():
+    """A face with boundary code 7 (neither connected nor wall) is skipped and
+    reported: into the caller's status word when one is given, else into the
+    sticky word that cb_noalloc_status reads and clears."""
+    import torch
+    from canary_b200._lib import CB_ERR_BC
+    m = dg.build_mesh(2, 3, (np.linspace(0.0, 10.0, 5),) * 2, (True, True))
+    X = m.coords()
+    U, V, rho, E = ic.isentropic_vortex(X[0], X[1])
+    Q = np.asfortranarray(np.stack([U, V, rho, E], axis=1))
+    dm = dg.DeviceMesh.upload(m)
+    bad = dm.elemtobndy.clone()
+    bad[5] = 7
+    q, r = dg.to_device(Q), torch.zeros(Q.size, dtype=torch.float64, device="cuda")
+    try:  # start from a clear sticky word whatever ran before in this process
+        dg.noalloc_status()
+    except CanaryError:
+        pass
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    dg.lsrk_stage_noalloc(2, 3, q, r, dm.vgeo, dm.sgeo, dm.vmapM, dm.vmapP, bad, dm.D, m.nelem,
+                          RKA[1], RKB[0], 1e-3, status=status)
+    torch.cuda.synchronize()
+    assert int(status.item()) & 1  # ST_BC into the caller's word
+    assert dg.noalloc_status() == 0  # ... and not into the sticky one
+    dg.lsrk_stage_noalloc(2, 3, q, r, dm.vgeo, dm.sgeo, dm.vmapM, dm.vmapP, bad, dm.D, m.nelem,
+                          RKA[1], RKB[0], 1e-3)
+    with pytest.raises(CanaryError) as ei:
+        dg.noalloc_status()
+    assert ei.value.code == CB_ERR_BC
+    assert dg.noalloc_status() == 0  # read and cleared
