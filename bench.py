@@ -500,6 +500,8 @@ def main():
     ap.add_argument("--precision", type=int, default=64, choices=[64, 32])
     ap.add_argument("--n-side", type=int, default=32)
     ap.add_argument("--order", type=int, default=7)
+    ap.add_argument("--stage-kernel", type=int, default=0, choices=[0, 1, 2],
+                    help="stage kernel: 0 default, 1 CUDA-core pipelined, 2 tensor-core (3-D N=7 FP64)")
     ap.add_argument("--ref-n-side", type=int, default=None,
                     help="mesh of the reference arm (default: --n-side, the same workload)")
     ap.add_argument("--e2e-steps", type=int, default=8)
@@ -537,6 +539,8 @@ def main():
     real = torch.float64 if args.precision == 64 else torch.float32
     solver = dg.LSRK(dm, dQ, drhs, args.precision, dg.make_phys(), stream)
     solver.set_offset(off)
+    solver.set_kernel(args.stage_kernel)
+    kernel_name = "k_stage_mma" if solver.kernel == 2 else "k_stage_pipe2"
     dof = mesh.nelem * mesh.Np * 5
     dQ0 = dQ.clone()  # initial state, for the parity run
 
@@ -579,6 +583,7 @@ def main():
     rhs2 = [drhs, torch.zeros_like(drhs)]
     solvers = [solver, dg.LSRK(dm, dQ2[1], rhs2[1], args.precision, dg.make_phys(), stream)]
     solvers[1].set_offset(off)
+    solvers[1].set_kernel(args.stage_kernel)
     up, down = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
     torch.cuda.synchronize(dev)
     if tdist is not None:
@@ -628,7 +633,7 @@ def main():
     t_launch = t_ms * 1e-3 / launches
     peak, peak_kind = measured_peaks()
     achieved = nodes * bpn / t_launch / 1e9
-    key = f"k_stage_3d_N{N}_fp{args.precision}_n{args.n_side}"
+    key = f"{kernel_name}_3d_N{N}_fp{args.precision}_n{args.n_side}"
     traffic = load_traffic(key)
     value = world * dof * 5 * args.steps / (t_ms * 1e-3)
     bi = dQ.numel() * w
@@ -646,7 +651,7 @@ def main():
                    "state_finite": finite},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
-                     "traffic": traffic, "bytes_per_node": bpn, "kernel": "k_stage_pipe2",
+                     "traffic": traffic, "bytes_per_node": bpn, "kernel": kernel_name,
                      "launch_ms": t_launch * 1e3},
         "e2e": {"value": world * dof * 5 * args.e2e_steps / (e2e_ms * 1e-3), "unit": METRIC,
                 "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo, "steps": args.e2e_steps,

@@ -25,7 +25,7 @@ EXPORTS = (
     "cb_volume_grad", "cb_flux_grad", "cb_update_gradQ", "cb_volume_div", "cb_flux_div",
     "cb_solver_create", "cb_lsrk_run", "cb_solver_set_offset", "cb_solver_sums",
     "cb_solver_destroy", "cb_solver_status_async", "cb_lsrk_stage_noalloc", "cb_noalloc_status",
-    "cb_solver_reset_status", "cb_solver_test_timeout",
+    "cb_solver_reset_status", "cb_solver_test_timeout", "cb_solver_set_kernel", "cb_solver_get_kernel",
     "cb_solver_create_ghosted", "cb_solver_stage", "cb_solver_stage_pass", "cb_solver_current", "cb_solver_settle",
     "cb_solver_pack", "cb_solver_unpack",
     "cb_computegeometry", "cb_brickmesh", "cb_mesh_create", "cb_mesh_affine", "cb_mesh_destroy",
@@ -115,6 +115,8 @@ def lib() -> C.CDLL:
     L.cb_solver_status_async.argtypes = [vp, vp]
     L.cb_solver_reset_status.argtypes = [vp]
     L.cb_solver_test_timeout.argtypes = [vp]
+    L.cb_solver_set_kernel.argtypes = [vp, C.c_int]
+    L.cb_solver_get_kernel.argtypes = [vp, C.POINTER(C.c_int)]
     _lib = L
     return L
 

@@ -436,6 +436,18 @@ class LSRK:
         tensor) on the solver's stream."""
         check(_lib.lib().cb_solver_status_async(self._h, C.c_void_p(host.data_ptr())))
 
+    def set_kernel(self, kernel: int) -> None:
+        """Stage kernel of the inviscid form: 0 = the shape's default, 1 = the
+        CUDA-core stages, 2 = the tensor-core (DMMA) stage of 3-D N=7 FP64."""
+        check(_lib.lib().cb_solver_set_kernel(self._h, int(kernel)))
+
+    @property
+    def kernel(self) -> int:
+        """The stage kernel the solver runs: 1 CUDA-core, 2 tensor-core."""
+        v = C.c_int(0)
+        check(_lib.lib().cb_solver_get_kernel(self._h, C.byref(v)))
+        return v.value
+
     def reset_status(self) -> None:
         """Clear the solver's sticky status bits (stream-ordered)."""
         check(_lib.lib().cb_solver_reset_status(self._h))

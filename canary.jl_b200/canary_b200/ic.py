@@ -158,9 +158,12 @@ def isentropic_vortex_t(x, y, beta=5.0, xc=5.0, yc=5.0, gamma=GAMMA):
 _FOURIER = {}
 
 
-def fourier_state_t(x, y, z, seed=0, kmax=4, gamma=GAMMA):
+def fourier_state_t(x, y, z, seed=0, kmax=4, gamma=GAMMA, vel_peak=None):
     """Torch form of fourier_state for device tensors x, y, z (FP64), summing
-    16 wave vectors per batch; returns (U, V, W, ρ, E) tensors."""
+    16 wave vectors per batch; returns (U, V, W, ρ, E) tensors.  With
+    `vel_peak`, each velocity component's Fourier sum is scaled so that its
+    largest magnitude over the given nodes is vel_peak (on the device, no
+    host synchronisation)."""
     import torch
     from .dg import to_device
     key = (kmax, str(x.device))
@@ -182,6 +185,8 @@ def fourier_state_t(x, y, z, seed=0, kmax=4, gamma=GAMMA):
         out.append(acc.reshape(x.shape))
     rho = 1.0 + out[0]
     u, v, w = out[1], out[2], out[3]
+    if vel_peak is not None:
+        u, v, w = (c * (vel_peak / torch.amax(torch.abs(c))) for c in (u, v, w))
     E = 1.0 / (gamma - 1.0) + 0.5 * rho * (u * u + v * v + w * w)
     return rho * u, rho * v, rho * w, rho, E
 

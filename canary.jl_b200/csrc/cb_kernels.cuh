@@ -758,6 +758,7 @@ __global__ void k_round_f32(float *__restrict__ dst, const double *__restrict__ 
 }  // namespace cb
 #include "cb_pipe.cuh"
 #include "cb_pipe2.cuh"
+#include "cb_mma.cuh"
 namespace cb {
 
 // ---------------------------------------------------------------- launchers
@@ -795,35 +796,68 @@ struct Launch {
                                                                 vmapP, bnd, p, status);
     return cudaGetLastError();
   }
-  // probe != 0: the timeout test hook of the pipelined stage (see MeshSrc);
-  // shapes without that stage return cudaErrorNotSupported for it.
+  // Whether the tensor-core (DMMA) stage is built for this shape.
+  static constexpr bool MMA_OK = DIM == 3 && Nq == 8 && sizeof(T) == 8;
+  // Whether kernel 0 (the shape's default) is the tensor-core stage: the
+  // faster of the two on B200 at the benchmark size.
+  static constexpr bool MMA_DEFAULT = MMA_OK && PipeM::DEFAULT;
+  // Resident blocks per SM of a kernel at `smem` bytes, from the occupancy
+  // calculator, cached per device in `cache`.
+  template <typename K>
+  static cudaError_t blocks_per_sm(K kernel, int threads, size_t smem, int *cache, int *out) {
+    int dev = 0;
+    cudaError_t err = cudaGetDevice(&dev);
+    if (err != cudaSuccess) return err;
+    if (dev < 0 || dev >= MAX_DEVICES) return cudaErrorInvalidDevice;
+    if (!cache[dev]) {
+      err = prep(kernel, smem);
+      if (err != cudaSuccess) return err;
+      int v = 0;
+      err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kernel, threads, smem);
+      if (err != cudaSuccess) return err;
+      cache[dev] = v < 1 ? 1 : v;
+    }
+    *out = cache[dev];
+    return cudaSuccess;
+  }
+  // kernel: 0 = the default for the shape (the tensor-core stage where it is
+  // built, else the pipelined CUDA-core stage, else the older ones), 1 = the
+  // CUDA-core stages only, 2 = the tensor-core stage (cudaErrorNotSupported
+  // where it is not built).  probe != 0: the timeout test hook of the
+  // pipelined stages (see MeshSrc); shapes without one return
+  // cudaErrorNotSupported for it.
   static cudaError_t stage(const T *Qin, T *Qout, T *rhs, const T *vgeo, const T *sgeo,
                            const int32_t *nbr, const T *D, int64_t nelem, const PhysT<T> &p,
                            const Offs<T, NS> &qref, T rka, T rkbdt, unsigned *status,
-                           cudaStream_t st, int probe = 0) {
+                           cudaStream_t st, int probe = 0, int kernel = 0) {
     constexpr bool pipe_ok = Pipe<DIM, Nq, T>::OK;
     const bool aligned = ((reinterpret_cast<uintptr_t>(Qin) | reinterpret_cast<uintptr_t>(vgeo)) & 15) == 0;
     const bool aligned2 = aligned && ((reinterpret_cast<uintptr_t>(rhs) | reinterpret_cast<uintptr_t>(sgeo)) & 15) == 0;
+    if (kernel == 2 && !(MMA_OK && aligned2)) return cudaErrorNotSupported;
+    if constexpr (MMA_OK) {
+      if ((kernel == 2 || (kernel == 0 && MMA_DEFAULT)) && aligned2) {
+        using S = MeshSrc<T, NS, C::EPB>;  // MeshSrc<double, 5, 1> here
+        static int per_sm[MAX_DEVICES] = {0};
+        int bps = 0;
+        cudaError_t err = blocks_per_sm(k_stage_mma<S, PipeM::MINB>, PipeM::THREADS, PipeM::smem(), per_sm, &bps);
+        if (err != cudaSuccess) return err;
+        int64_t g = (int64_t)num_sms() * bps;
+        if (g > nelem) g = nelem;
+        const S src{Qin, Qout, rhs, vgeo, sgeo, nbr, D, nelem, qref, rkbdt, status, probe};
+        k_stage_mma<S, PipeM::MINB><<<(int)g, PipeM::THREADS, PipeM::smem(), st>>>(src, p, rka);
+        return cudaGetLastError();
+      }
+    }
     if (Pipe2<DIM, Nq, T>::OK && aligned2) {
       using PP = Pipe2<DIM, Nq, T>;
       using S = MeshSrc<T, NS, C::EPB>;
       const size_t sm = PP::smem();
-      // resident blocks per SM, from the occupancy calculator, per device
       static int per_sm[MAX_DEVICES] = {0};
-      int dev = 0;
-      cudaError_t err = cudaGetDevice(&dev);
+      int bps = 0;
+      cudaError_t err = blocks_per_sm(k_stage_pipe2<DIM, Nq, T, S>, C::THREADS, sm, per_sm, &bps);
       if (err != cudaSuccess) return err;
-      if (dev < 0 || dev >= MAX_DEVICES) return cudaErrorInvalidDevice;
-      if (!per_sm[dev]) {
-        err = prep(k_stage_pipe2<DIM, Nq, T, S>, sm);
-        if (err != cudaSuccess) return err;
-        int v = 0;
-        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_stage_pipe2<DIM, Nq, T, S>, C::THREADS, sm);
-        if (err != cudaSuccess) return err;
-        per_sm[dev] = v < 1 ? 1 : v;
-      }
       const int64_t groups = (nelem + C::EPB - 1) / C::EPB;
-      int64_t g = (int64_t)num_sms() * per_sm[dev];
+      int64_t g = (int64_t)num_sms() * bps;
       if (g > groups) g = groups;
       const S src{Qin, Qout, rhs, vgeo, sgeo, nbr, D, nelem, qref, rkbdt, status, probe};
       k_stage_pipe2<DIM, Nq, T, S><<<(int)g, C::THREADS, sm, st>>>(src, p, rka);

@@ -20,11 +20,15 @@ struct Ops {
                          const int64_t *, const int64_t *, const PhysT<T> &, unsigned *, cudaStream_t);
   cudaError_t (*stage)(const T *, T *, T *, const T *, const T *, const int32_t *, const T *, int64_t,
                        const PhysT<T> &, const Offs<T, 5> &, T, T, unsigned *, cudaStream_t);
-  // the stage as the timeout test hook: the pipelined stage with each block's
-  // first state copy withheld and a short wait limit (cudaErrorNotSupported
-  // where the pipelined stage does not run)
-  cudaError_t (*stage_probe)(const T *, T *, T *, const T *, const T *, const int32_t *, const T *, int64_t,
-                             const PhysT<T> &, const Offs<T, 5> &, T, T, unsigned *, cudaStream_t);
+  // the stage with a kernel choice (last argument: 0 the shape's default,
+  // 1 the CUDA-core stages, 2 the tensor-core stage; cudaErrorNotSupported
+  // where the choice is not built) and, before it, the timeout test hook
+  // flag (each block's first state copy withheld and a short wait limit;
+  // cudaErrorNotSupported where no pipelined stage runs)
+  cudaError_t (*stage_k)(const T *, T *, T *, const T *, const T *, const int32_t *, const T *, int64_t,
+                         const PhysT<T> &, const Offs<T, 5> &, T, T, unsigned *, cudaStream_t, int, int);
+  bool mma;          // whether the tensor-core stage is built for this shape
+  bool mma_default;  // whether it is the shape's default stage kernel
   cudaError_t (*build_nbr)(int32_t *, const int64_t *, const int64_t *, const int64_t *, int64_t,
                            unsigned *, cudaStream_t);
   // the same with neighbours allowed up to a total element count (ghosts)

@@ -49,6 +49,7 @@ struct cb_solver {
   double qref[5] = {0, 0, 0, 0, 0};  // stored state = Q - qref
   int64_t nghost = 0;  // ghost elements after the nelem own ones in Q and the twin
   int cur = 0;         // stage API: the current state is in Q (0) or in the twin (1)
+  int kernel = 0;      // stage kernel choice (cb_solver_set_kernel)
 };
 
 namespace {
@@ -117,8 +118,8 @@ cudaError_t enqueue_step(cb_solver *s, double dt, bool from_user) {
   Offs<T, 5> q5;
   for (int k = 0; k < 5; ++k) q5.v[k] = T(s->qref[k]);
   for (int st = 0; st < 5 && e == cudaSuccess; ++st) {
-    e = o->stage(a, b, (T *)s->rhs, vg, sg, s->nbr, D, s->nelem, p, q5, T(RKA[(st + 1) % 5]),
-                 T(RKB[st] * dt), s->status, s->stream);
+    e = o->stage_k(a, b, (T *)s->rhs, vg, sg, s->nbr, D, s->nelem, p, q5, T(RKA[(st + 1) % 5]),
+                   T(RKB[st] * dt), s->status, s->stream, 0, s->kernel);
     T *t = a;
     a = b;
     b = t;
@@ -203,8 +204,8 @@ cudaError_t enqueue_pass(cb_solver *s, int st, double dt, int pass) {
   if (pass == 0) return cudaSuccess;
   Offs<T, 5> q5;
   for (int k = 0; k < 5; ++k) q5.v[k] = T(s->qref[k]);
-  return o->stage(a, b, (T *)s->rhs, (const T *)s->vgeo, (const T *)s->sgeo, s->nbr, (const T *)s->D, s->nelem, p,
-                  q5, T(RKA[(st + 1) % 5]), T(RKB[st] * dt), s->status, s->stream);
+  return o->stage_k(a, b, (T *)s->rhs, (const T *)s->vgeo, (const T *)s->sgeo, s->nbr, (const T *)s->D, s->nelem,
+                    p, q5, T(RKA[(st + 1) % 5]), T(RKB[st] * dt), s->status, s->stream, 0, s->kernel);
 }
 
 // Copy whole elements: gather `n` elements listed in `idx` (device int64) of
@@ -487,6 +488,26 @@ int cb_solver_set_offset(cb_solver *s, const double *qref) {
   return CB_OK;
 }
 
+int cb_solver_set_kernel(cb_solver *s, int kernel) {
+  if (!s || kernel < 0 || kernel > 2) return solver_fail(CB_ERR_ARG, "cb_solver_set_kernel: bad arguments");
+  if (kernel == 2) {
+    const bool mma = s->prec == 64 ? ops<double>(s)->mma : ops<float>(s)->mma;
+    if (!mma || s->phys.visc > 0)
+      return solver_fail(CB_ERR_UNSUPPORTED,
+                         "cb_solver_set_kernel: the tensor-core stage is built for the inviscid 3-D N=7 FP64 form");
+  }
+  if (kernel != s->kernel) drop_graph(s);
+  s->kernel = kernel;
+  return CB_OK;
+}
+
+int cb_solver_get_kernel(const cb_solver *s, int *kernel) {
+  if (!s || !kernel) return solver_fail(CB_ERR_ARG, "cb_solver_get_kernel: null argument");
+  const bool mma_def = s->prec == 64 ? ops<double>(s)->mma_default : ops<float>(s)->mma_default;
+  *kernel = s->kernel ? s->kernel : (mma_def && s->phys.visc <= 0 ? 2 : 1);
+  return CB_OK;
+}
+
 int cb_solver_reset_status(cb_solver *s) {
   if (!s) return solver_fail(CB_ERR_ARG, "cb_solver_reset_status: null solver");
   const cudaError_t e = cudaMemsetAsync(s->status, 0, sizeof(unsigned), s->stream);
@@ -506,15 +527,15 @@ int cb_solver_test_timeout(cb_solver *s) {
   if (s->prec == 64) {
     Offs<double, 5> q5;
     for (int k = 0; k < 5; ++k) q5.v[k] = s->qref[k];
-    e = ops<double>(s)->stage_probe((const double *)a, (double *)b, (double *)s->rhs, (const double *)s->vgeo,
-                                    (const double *)s->sgeo, s->nbr, (const double *)s->D, s->nelem, p64, q5,
-                                    RKA[1], RKB[0], s->status, s->stream);
+    e = ops<double>(s)->stage_k((const double *)a, (double *)b, (double *)s->rhs, (const double *)s->vgeo,
+                                (const double *)s->sgeo, s->nbr, (const double *)s->D, s->nelem, p64, q5, RKA[1],
+                                RKB[0], s->status, s->stream, 1, s->kernel);
   } else {
     Offs<float, 5> q5;
     for (int k = 0; k < 5; ++k) q5.v[k] = (float)s->qref[k];
-    e = ops<float>(s)->stage_probe((const float *)a, (float *)b, (float *)s->rhs, (const float *)s->vgeo,
-                                   (const float *)s->sgeo, s->nbr, (const float *)s->D, s->nelem, p32, q5,
-                                   (float)RKA[1], (float)RKB[0], s->status, s->stream);
+    e = ops<float>(s)->stage_k((const float *)a, (float *)b, (float *)s->rhs, (const float *)s->vgeo,
+                               (const float *)s->sgeo, s->nbr, (const float *)s->D, s->nelem, p32, q5,
+                               (float)RKA[1], (float)RKB[0], s->status, s->stream, 1, s->kernel);
   }
   if (e == cudaErrorNotSupported)  // returned by the launcher, not by CUDA
     return solver_fail(CB_ERR_UNSUPPORTED, "cb_solver_test_timeout: this shape does not run the pipelined stage");

@@ -184,6 +184,16 @@ int cb_solver_sums(cb_solver *s, double *out_host);
  * non-finite state) into *out_host (page-locked memory for an asynchronous
  * copy); the value is valid once the stream has reached the copy. */
 int cb_solver_status_async(cb_solver *s, unsigned *out_host);
+/* Stage kernel of the inviscid form: 0 = the default for the shape, 1 = the
+ * CUDA-core stages (pipelined bulk-copy staging where the plan fits), 2 = the
+ * tensor-core stage (D contraction on the FP64 tensor pipe as 8x8x4 DMMA
+ * tiles; built for 3-D N=7 FP64, CB_ERR_UNSUPPORTED elsewhere).  The default
+ * is whichever of the two is faster on B200 for the shape.  Both agree with
+ * the oracle to round-off; changing it re-captures the step graph at the
+ * next run.
+ * cb_solver_get_kernel reports the kernel the solver runs (1 or 2). */
+int cb_solver_set_kernel(cb_solver *s, int kernel);
+int cb_solver_get_kernel(const cb_solver *s, int *kernel);
 /* Clear the solver's sticky status bits (stream-ordered). */
 int cb_solver_reset_status(cb_solver *s);
 /* Test hook of the bounded waits (no counterpart in the reference): enqueue
@@ -318,8 +328,11 @@ int cb_batch_set_variant(cb_batch *b, int dim, int N, int variant);
 int cb_batch_get_variant(const cb_batch *b, int dim, int N, int *variant);
 /* Instances admitted from now on whose mesh is affine (cb_mesh_affine), with
  * gravity 0 and a pipelined variant selected, use the affine-element stage
- * when `on` (the default); it agrees with the per-node geometry to
- * round-off and reads no vgeo / sgeo. */
+ * when `on`; it reads no vgeo / sgeo and uses each element's first-node
+ * metric for all its nodes, which agrees with the per-node geometry to
+ * round-off per stage.  Default: on for precision 32, off for precision 64
+ * (over hundreds of FP64 steps that round-off reaches ~1e-11 relative,
+ * above the 1e-12 oracle bar). */
 int cb_batch_set_affine(cb_batch *b, int on);
 /* Admit an instance: the caller's state Q and zeroed residual carry rhs
  * (layouts as above, precision of the batch) advance by nsteps steps of dt

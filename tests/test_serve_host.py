@@ -57,3 +57,38 @@ def test_mesh_pool_evicts_idle_meshes_least_recently_used_first():
     assert not pool.evict(need=80, budget=100, in_use=0)     # "b" is in use: cannot make room
     assert set(pool.meshes) == {"b"} and _BM.closed == 2
     assert S.MeshPool.nbytes(3, 3, 4, 32) > S.MeshPool.nbytes(3, 3, 4, 64) > 0
+
+
+def test_report_counts_completed_requests_only():
+    lat = {0: 1.0, 1: 2.0, 2: 30.0, 3: 4.0}
+    kinds = {0: "vortex", 1: "vortex", 2: "euler3d", 3: "ns3d", 4: "euler3d", 5: "vortex"}
+    rep = S.Report(lat, {}, 0.0, 10.0, 1e12, 0, 3, failed={2}, kinds=kinds, rejected={4: "too big"},
+                   cancelled={5}, work={0: 1e10, 1: 2e10, 3: 3e10})
+    s = rep.summary()
+    assert s["requests"] == 6 and s["completed"] == 3
+    assert s["failed"] == 1 and s["rejected"] == 1 and s["cancelled"] == 1
+    assert s["solves_per_s"] == 3 / 10.0
+    assert s["p50_s"] == 2.0 and s["p99_s"] < 4.0 + 1e-9  # the failed request's 30 s is not counted
+    assert s["dof_stage_per_s"] == 1e11 and s["completed_dof_stage_per_s"] == 6e9
+    pk = s["per_kind"]
+    assert pk["vortex"]["completed"] == 2 and pk["vortex"]["cancelled"] == 1
+    assert pk["euler3d"]["completed"] == 0 and pk["euler3d"]["failed"] == 1 and pk["euler3d"]["rejected"] == 1
+    assert np.isnan(pk["euler3d"]["p50_s"]) and pk["ns3d"]["p50_s"] == 4.0
+
+
+def test_request_that_can_never_fit_is_recognised():
+    import types
+    srv = types.SimpleNamespace(precision=32, budget=2 * 10 ** 8)
+    srv.request_bytes = lambda r: S.Server.request_bytes(srv, r)
+    small = S.Request(0, "vortex", 3, 8, 0.5, 0.0)
+    big = S.Request(1, "euler3d", 7, 16, 0.5, 0.0)
+    assert not S.Server.never_fits(srv, small)
+    assert S.Server.never_fits(srv, big)  # 16^3 N=7: state and mesh exceed 200 MB
+
+
+def test_normalised_stream_scales_only_the_3d_requests():
+    a = S.request_stream(50, rate=10.0, seed=1)
+    b = S.request_stream(50, rate=10.0, seed=1, vel_peak=0.1)
+    for r, q in zip(a, b):
+        assert (r.kind, r.N, r.n_side, r.t_final, r.arrival) == (q.kind, q.N, q.n_side, q.t_final, q.arrival)
+        assert r.vel_peak is None and q.vel_peak == (None if q.dim == 2 else 0.1)
