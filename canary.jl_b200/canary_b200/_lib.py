@@ -27,7 +27,8 @@ EXPORTS = (
     "cb_solver_destroy", "cb_solver_status_async", "cb_lsrk_stage_noalloc", "cb_noalloc_status",
     "cb_solver_reset_status", "cb_solver_test_timeout", "cb_solver_set_kernel", "cb_solver_get_kernel",
     "cb_solver_create_ghosted", "cb_solver_stage", "cb_solver_stage_pass", "cb_solver_current", "cb_solver_settle",
-    "cb_solver_pack", "cb_solver_unpack",
+    "cb_solver_pack", "cb_solver_unpack", "cb_solver_pack_faces", "cb_solver_unpack_faces",
+    "cb_solver_set_split", "cb_solver_stage_split",
     "cb_computegeometry", "cb_brickmesh", "cb_mesh_create", "cb_mesh_affine", "cb_mesh_destroy",
     "cb_batch_create", "cb_batch_set_variant", "cb_batch_get_variant", "cb_batch_set_affine",
     "cb_batch_slot_variant", "cb_batch_add",
@@ -92,6 +93,10 @@ def lib() -> C.CDLL:
     L.cb_solver_settle.argtypes = [vp]
     L.cb_solver_pack.argtypes = [vp, C.c_int, vp, i64, vp]
     L.cb_solver_unpack.argtypes = [vp, C.c_int, vp, i64, i64]
+    L.cb_solver_pack_faces.argtypes = [vp, C.c_int, vp, i64, vp]
+    L.cb_solver_unpack_faces.argtypes = [vp, C.c_int, vp, i64, vp]
+    L.cb_solver_set_split.argtypes = [vp, i64]
+    L.cb_solver_stage_split.argtypes = [vp, C.c_int, dbl, C.c_int, C.POINTER(vp)]
     L.cb_lsrk_stage_noalloc.argtypes = [C.c_int, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp, i64,
                                         phys_p, dbl, dbl, dbl, vp, vp]
     L.cb_noalloc_status.argtypes = [vp, C.POINTER(C.c_uint)]

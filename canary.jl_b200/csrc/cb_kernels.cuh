@@ -826,14 +826,20 @@ struct Launch {
   // where it is not built).  probe != 0: the timeout test hook of the
   // pipelined stages (see MeshSrc); shapes without one return
   // cudaErrorNotSupported for it.
+  // ebeg: the launch covers elements ebeg .. nelem - 1 (neighbour indices
+  // stay absolute); only the pipelined and tensor-core stages take ebeg > 0,
+  // the others return cudaErrorNotSupported for it.
   static cudaError_t stage(const T *Qin, T *Qout, T *rhs, const T *vgeo, const T *sgeo,
                            const int32_t *nbr, const T *D, int64_t nelem, const PhysT<T> &p,
                            const Offs<T, NS> &qref, T rka, T rkbdt, unsigned *status,
-                           cudaStream_t st, int probe = 0, int kernel = 0) {
+                           cudaStream_t st, int probe = 0, int kernel = 0, int64_t ebeg = 0) {
     constexpr bool pipe_ok = Pipe<DIM, Nq, T>::OK;
     const bool aligned = ((reinterpret_cast<uintptr_t>(Qin) | reinterpret_cast<uintptr_t>(vgeo)) & 15) == 0;
     const bool aligned2 = aligned && ((reinterpret_cast<uintptr_t>(rhs) | reinterpret_cast<uintptr_t>(sgeo)) & 15) == 0;
     if (kernel == 2 && !(MMA_OK && aligned2)) return cudaErrorNotSupported;
+    if (ebeg < 0 || ebeg > nelem) return cudaErrorInvalidValue;
+    const int64_t groups = (nelem - ebeg + C::EPB - 1) / C::EPB;
+    if (groups == 0) return cudaSuccess;
     if constexpr (MMA_OK) {
       if ((kernel == 2 || (kernel == 0 && MMA_DEFAULT)) && aligned2) {
         using S = MeshSrc<T, NS, C::EPB>;  // MeshSrc<double, 5, 1> here
@@ -842,8 +848,8 @@ struct Launch {
         cudaError_t err = blocks_per_sm(k_stage_mma<S, PipeM::MINB>, PipeM::THREADS, PipeM::smem(), per_sm, &bps);
         if (err != cudaSuccess) return err;
         int64_t g = (int64_t)num_sms() * bps;
-        if (g > nelem) g = nelem;
-        const S src{Qin, Qout, rhs, vgeo, sgeo, nbr, D, nelem, qref, rkbdt, status, probe};
+        if (g > groups) g = groups;
+        const S src{Qin, Qout, rhs, vgeo, sgeo, nbr, D, nelem, qref, rkbdt, status, probe, ebeg};
         k_stage_mma<S, PipeM::MINB><<<(int)g, PipeM::THREADS, PipeM::smem(), st>>>(src, p, rka);
         return cudaGetLastError();
       }
@@ -856,20 +862,18 @@ struct Launch {
       int bps = 0;
       cudaError_t err = blocks_per_sm(k_stage_pipe2<DIM, Nq, T, S>, C::THREADS, sm, per_sm, &bps);
       if (err != cudaSuccess) return err;
-      const int64_t groups = (nelem + C::EPB - 1) / C::EPB;
       int64_t g = (int64_t)num_sms() * bps;
       if (g > groups) g = groups;
-      const S src{Qin, Qout, rhs, vgeo, sgeo, nbr, D, nelem, qref, rkbdt, status, probe};
+      const S src{Qin, Qout, rhs, vgeo, sgeo, nbr, D, nelem, qref, rkbdt, status, probe, ebeg};
       k_stage_pipe2<DIM, Nq, T, S><<<(int)g, C::THREADS, sm, st>>>(src, p, rka);
       return cudaGetLastError();
-    } else if (probe) {
+    } else if (probe || ebeg) {
       return cudaErrorNotSupported;
     } else if (pipe_ok && aligned) {
       using PP = Pipe<DIM, Nq, T>;
       size_t sm = PP::smem();
       cudaError_t err = prep(k_stage_pipe<DIM, Nq, T>, sm);
       if (err != cudaSuccess) return err;
-      const int64_t groups = (nelem + C::EPB - 1) / C::EPB;
       int g = num_sms();
       if ((int64_t)g > groups) g = (int)groups;
       k_stage_pipe<DIM, Nq, T><<<g, C::THREADS, sm, st>>>(Qin, Qout, rhs, vgeo, sgeo, nbr, D, nelem,
@@ -883,6 +887,13 @@ struct Launch {
                                                                 nelem, p, qref, rka, rkbdt, status);
       return cudaGetLastError();
     }
+  }
+  // Whether stage() takes an element range (ebeg > 0) for arrays aligned
+  // like these.
+  static bool ranged(const void *Qin, const void *rhs, const void *vgeo, const void *sgeo) {
+    const bool a = ((reinterpret_cast<uintptr_t>(Qin) | reinterpret_cast<uintptr_t>(rhs) |
+                     reinterpret_cast<uintptr_t>(vgeo) | reinterpret_cast<uintptr_t>(sgeo)) & 15) == 0;
+    return a && (Pipe2<DIM, Nq, T>::OK || MMA_OK);
   }
   static cudaError_t build_nbr(int32_t *nbr, const int64_t *vmapM, const int64_t *vmapP,
                                const int64_t *bnd, int64_t nelem, unsigned *status,

@@ -20,13 +20,17 @@ struct Ops {
                          const int64_t *, const int64_t *, const PhysT<T> &, unsigned *, cudaStream_t);
   cudaError_t (*stage)(const T *, T *, T *, const T *, const T *, const int32_t *, const T *, int64_t,
                        const PhysT<T> &, const Offs<T, 5> &, T, T, unsigned *, cudaStream_t);
-  // the stage with a kernel choice (last argument: 0 the shape's default,
-  // 1 the CUDA-core stages, 2 the tensor-core stage; cudaErrorNotSupported
-  // where the choice is not built) and, before it, the timeout test hook
-  // flag (each block's first state copy withheld and a short wait limit;
-  // cudaErrorNotSupported where no pipelined stage runs)
+  // the stage with, after the stream: the timeout test hook flag (each
+  // block's first state copy withheld and a short wait limit;
+  // cudaErrorNotSupported where no pipelined stage runs), the kernel choice
+  // (0 the shape's default, 1 the CUDA-core stages, 2 the tensor-core stage;
+  // cudaErrorNotSupported where the choice is not built) and the first
+  // element of the launch (elements first .. nelem - 1)
   cudaError_t (*stage_k)(const T *, T *, T *, const T *, const T *, const int32_t *, const T *, int64_t,
-                         const PhysT<T> &, const Offs<T, 5> &, T, T, unsigned *, cudaStream_t, int, int);
+                         const PhysT<T> &, const Offs<T, 5> &, T, T, unsigned *, cudaStream_t, int, int, int64_t);
+  // whether stage_k takes a first element > 0 (an element range) for arrays
+  // aligned like these: (Qin, rhs, vgeo, sgeo)
+  bool (*ranged)(const void *, const void *, const void *, const void *);
   bool mma;          // whether the tensor-core stage is built for this shape
   bool mma_default;  // whether it is the shape's default stage kernel
   cudaError_t (*build_nbr)(int32_t *, const int64_t *, const int64_t *, const int64_t *, int64_t,

@@ -115,15 +115,20 @@ struct MeshSrc {
   // first group is never issued and waits give up after PROBE_WAIT_LIMIT
   // polls, so that the bounded wait runs out on an mbarrier nobody arrives on.
   int probe_;
+  // The launch covers elements ebeg_ .. nelem - 1 (a partitioned solve runs
+  // the elements that read no ghost first, the others once ghosts arrived).
+  int64_t ebeg_;
   __device__ bool skip_copy(int it) const { return probe_ != 0 && it == 0; }
   __device__ uint32_t wait_limit() const { return probe_ ? PROBE_WAIT_LIMIT : WAIT_LIMIT; }
   __device__ void begin(unsigned char *) {}
   __device__ void prefetch() {}
   __device__ void publish(int) {}
   __device__ int64_t g(int it) const { return (int64_t)blockIdx.x + (int64_t)it * gridDim.x; }
-  __device__ bool valid(int it) const { return g(it) * EPB < nelem; }
-  __device__ bool last(int it) const { return (g(it) + 1) * EPB >= nelem; }  // the group ends the arrays
-  __device__ int64_t e0(int it) const { return g(it) * EPB; }
+  __device__ bool valid(int it) const { return e0(it) < nelem; }
+  // the group ends the launch's range (taken as the end of the arrays: the
+  // last bytes are then loaded with plain loads, which is safe either way)
+  __device__ bool last(int it) const { return e0(it) + EPB >= nelem; }
+  __device__ int64_t e0(int it) const { return ebeg_ + g(it) * EPB; }
   __device__ int nv(int it) const {
     const int64_t r = nelem - e0(it);
     return r < EPB ? (int)r : EPB;

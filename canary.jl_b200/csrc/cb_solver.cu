@@ -50,6 +50,7 @@ struct cb_solver {
   int64_t nghost = 0;  // ghost elements after the nelem own ones in Q and the twin
   int cur = 0;         // stage API: the current state is in Q (0) or in the twin (1)
   int kernel = 0;      // stage kernel choice (cb_solver_set_kernel)
+  int64_t nsplit = -1;  // elements 0 .. nsplit - 1 read no ghost (cb_solver_set_split); -1: not set
 };
 
 namespace {
@@ -119,7 +120,7 @@ cudaError_t enqueue_step(cb_solver *s, double dt, bool from_user) {
   for (int k = 0; k < 5; ++k) q5.v[k] = T(s->qref[k]);
   for (int st = 0; st < 5 && e == cudaSuccess; ++st) {
     e = o->stage_k(a, b, (T *)s->rhs, vg, sg, s->nbr, D, s->nelem, p, q5, T(RKA[(st + 1) % 5]),
-                   T(RKB[st] * dt), s->status, s->stream, 0, s->kernel);
+                   T(RKB[st] * dt), s->status, s->stream, 0, s->kernel, 0);
     T *t = a;
     a = b;
     b = t;
@@ -205,7 +206,7 @@ cudaError_t enqueue_pass(cb_solver *s, int st, double dt, int pass) {
   Offs<T, 5> q5;
   for (int k = 0; k < 5; ++k) q5.v[k] = T(s->qref[k]);
   return o->stage_k(a, b, (T *)s->rhs, (const T *)s->vgeo, (const T *)s->sgeo, s->nbr, (const T *)s->D, s->nelem,
-                    p, q5, T(RKA[(st + 1) % 5]), T(RKB[st] * dt), s->status, s->stream, 0, s->kernel);
+                    p, q5, T(RKA[(st + 1) % 5]), T(RKB[st] * dt), s->status, s->stream, 0, s->kernel, 0);
 }
 
 // Copy whole elements: gather `n` elements listed in `idx` (device int64) of
@@ -217,9 +218,117 @@ __global__ void k_pack(const T *__restrict__ src, const int64_t *__restrict__ id
     dst[t] = src[idx[t / ew] * ew + t % ew];
 }
 
+// Face traces of a partitioned solve.  Entry i of `codes` is (element << 3) |
+// face; an entry carries the Nfp face-node values of W components (the
+// state's fields, or state field x direction for the gradient), each
+// component at element offset Np·c.  Pack reads own elements (0 .. nown - 1)
+// into buf[(i·W + c)·Nfp + fn]; unpack writes ghost slots (element nown + g
+// for code g << 3 | face).  An entry out of range is skipped and raises
+// ST_MESH.
+template <int DIM, typename T>
+__global__ void k_faces(bool pack, T *__restrict__ arr, const int64_t *__restrict__ codes, int64_t n, int Nq,
+                        int W, int64_t nown, int64_t nghost, T *__restrict__ buf, unsigned *status) {
+  const int Nfp = DIM == 2 ? Nq : Nq * Nq, Np = Nfp * Nq;
+  const int64_t per = (int64_t)W * Nfp;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n * per; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = t / per;
+    const int c = (int)((t % per) / Nfp), fn = (int)(t % Nfp);
+    const int64_t code = codes[i], e = code >> 3;
+    const int f = (int)(code & 7);
+    if (e < 0 || f >= 2 * DIM || e >= (pack ? nown : nghost)) {
+      if (c == 0 && fn == 0) atomicOr(status, ST_MESH);
+      continue;
+    }
+    const int64_t el = pack ? e : nown + e;
+    T *a = arr + face_node_rt<DIM>(Nq, f, fn) + (int64_t)Np * (c + (int64_t)W * el);
+    if (pack) buf[t] = *a;
+    else *a = buf[t];
+  }
+}
+
+template <typename T>
+cudaError_t launch_faces(const cb_solver *s, bool pack, int what, const int64_t *codes, int64_t n, void *buf) {
+  const int Nq = s->N + 1, Nfp = s->dim == 2 ? Nq : Nq * Nq;
+  const int W = (s->dim == 2 ? 4 : 5) * (what ? s->dim : 1);
+  T *arr = (T *)(what ? s->gradQ : (s->cur ? s->Qalt : s->Q));
+  const int64_t total = n * W * Nfp;
+  const int grid = (int)std::min<int64_t>((total + 255) / 256, 148 * 16);
+  if (s->dim == 2)
+    k_faces<2, T><<<grid, 256, 0, s->stream>>>(pack, arr, codes, n, Nq, W, s->nelem, s->nghost, (T *)buf, s->status);
+  else
+    k_faces<3, T><<<grid, 256, 0, s->stream>>>(pack, arr, codes, n, Nq, W, s->nelem, s->nghost, (T *)buf, s->status);
+  return cudaGetLastError();
+}
+
+int faces(cb_solver *s, bool pack, int what, const int64_t *codes, int64_t n, void *buf) {
+  const char *who = pack ? "cb_solver_pack_faces" : "cb_solver_unpack_faces";
+  if (!s || n < 0 || (n && (!codes || !buf)) || what < 0 || what > 1 || (what == 1 && !s->gradQ))
+    return solver_fail(CB_ERR_ARG, "%s: bad arguments", who);
+  if (!n) return CB_OK;
+  const cudaError_t e = s->prec == 64 ? launch_faces<double>(s, pack, what, codes, n, buf)
+                                      : launch_faces<float>(s, pack, what, codes, n, buf);
+  return e == cudaSuccess ? CB_OK : solver_fail(CB_ERR_CUDA, "%s: %s", who, cudaGetErrorString(e));
+}
+
 }  // namespace
 
 extern "C" {
+
+int cb_solver_pack_faces(cb_solver *s, int what, const int64_t *codes, int64_t n, void *buf) {
+  return faces(s, true, what, codes, n, buf);
+}
+
+int cb_solver_unpack_faces(cb_solver *s, int what, const int64_t *codes, int64_t n, void *buf) {
+  return faces(s, false, what, codes, n, buf);
+}
+
+int cb_solver_set_split(cb_solver *s, int64_t ninterior) {
+  if (!s || ninterior < 0 || ninterior > s->nelem)
+    return solver_fail(CB_ERR_ARG, "cb_solver_set_split: the split must be within 0..nelem");
+  if (s->phys.visc > 0)
+    return solver_fail(CB_ERR_UNSUPPORTED, "cb_solver_set_split: the inviscid form only");
+  const void *Qa = s->Q, *Qb = s->Qalt;
+  const bool ok = s->prec == 64 ? ops<double>(s)->ranged(Qa, s->rhs, s->vgeo, s->sgeo) &&
+                                      ops<double>(s)->ranged(Qb, s->rhs, s->vgeo, s->sgeo)
+                                : ops<float>(s)->ranged(Qa, s->rhs, s->vgeo, s->sgeo) &&
+                                      ops<float>(s)->ranged(Qb, s->rhs, s->vgeo, s->sgeo);
+  if (!ok)
+    return solver_fail(CB_ERR_UNSUPPORTED,
+                       "cb_solver_set_split: this shape's stage does not run over element ranges");
+  s->nsplit = ninterior;
+  return CB_OK;
+}
+
+int cb_solver_stage_split(cb_solver *s, int stage, double dt, int half, void **next_in) {
+  if (!s || stage < 0 || stage > 4 || half < 0 || half > 1)
+    return solver_fail(CB_ERR_ARG, "cb_solver_stage_split: bad arguments");
+  if (s->nsplit < 0) return solver_fail(CB_ERR_ARG, "cb_solver_stage_split: no split set (cb_solver_set_split)");
+  const int64_t lo = half ? s->nsplit : 0, hi = half ? s->nelem : s->nsplit;
+  cudaError_t e = cudaSuccess;
+  if (hi > lo) {
+    void *a = s->cur ? s->Qalt : s->Q, *b = s->cur ? s->Q : s->Qalt;
+    const Phys ph{s->phys.gamma, s->phys.R_gas, s->phys.c_p, s->phys.c_v, s->phys.gravity, s->phys.Pr,
+                  s->phys.lambda, s->phys.visc};
+    if (s->prec == 64) {
+      Offs<double, 5> q5;
+      for (int k = 0; k < 5; ++k) q5.v[k] = s->qref[k];
+      e = ops<double>(s)->stage_k((const double *)a, (double *)b, (double *)s->rhs, (const double *)s->vgeo,
+                                  (const double *)s->sgeo, s->nbr, (const double *)s->D, hi, PhysT<double>(ph), q5,
+                                  RKA[(stage + 1) % 5], RKB[stage] * dt, s->status, s->stream, 0, s->kernel, lo);
+    } else {
+      Offs<float, 5> q5;
+      for (int k = 0; k < 5; ++k) q5.v[k] = (float)s->qref[k];
+      e = ops<float>(s)->stage_k((const float *)a, (float *)b, (float *)s->rhs, (const float *)s->vgeo,
+                                 (const float *)s->sgeo, s->nbr, (const float *)s->D, hi, PhysT<float>(ph), q5,
+                                 (float)RKA[(stage + 1) % 5], (float)(RKB[stage] * dt), s->status, s->stream, 0,
+                                 s->kernel, lo);
+    }
+  }
+  if (e != cudaSuccess) return solver_fail(CB_ERR_CUDA, "cb_solver_stage_split: %s", cudaGetErrorString(e));
+  if (half == 1) s->cur ^= 1;
+  if (next_in) *next_in = s->cur ? s->Qalt : s->Q;
+  return CB_OK;
+}
 
 int cb_solver_create(cb_solver **out, int dim, int N, int precision, int64_t nelem, void *Q,
                      void *rhs, const double *vgeo, const double *sgeo, const int64_t *vmapM,
@@ -234,6 +343,10 @@ int cb_solver_create_ghosted(cb_solver **out, int dim, int N, int precision, int
                              const int64_t *vmapP, const int64_t *elemtobndy, const double *D,
                              const cb_phys *phys, cb_stream_t stream) {
   if (nghost < 0) return solver_fail(CB_ERR_ARG, "cb_solver_create_ghosted: nghost must be >= 0");
+  // the gravity source reads the neighbour's height from vgeo, which holds
+  // the own elements only
+  if (nghost > 0 && phys && phys->gravity != 0.0)
+    return solver_fail(CB_ERR_UNSUPPORTED, "cb_solver_create_ghosted: ghost elements with gravity != 0");
   return solver_create(out, dim, N, precision, nelem, nghost, Q, rhs, vgeo, sgeo, vmapM, vmapP, elemtobndy, D,
                        phys, stream);
 }
@@ -529,13 +642,13 @@ int cb_solver_test_timeout(cb_solver *s) {
     for (int k = 0; k < 5; ++k) q5.v[k] = s->qref[k];
     e = ops<double>(s)->stage_k((const double *)a, (double *)b, (double *)s->rhs, (const double *)s->vgeo,
                                 (const double *)s->sgeo, s->nbr, (const double *)s->D, s->nelem, p64, q5, RKA[1],
-                                RKB[0], s->status, s->stream, 1, s->kernel);
+                                RKB[0], s->status, s->stream, 1, s->kernel, 0);
   } else {
     Offs<float, 5> q5;
     for (int k = 0; k < 5; ++k) q5.v[k] = (float)s->qref[k];
     e = ops<float>(s)->stage_k((const float *)a, (float *)b, (float *)s->rhs, (const float *)s->vgeo,
                                (const float *)s->sgeo, s->nbr, (const float *)s->D, s->nelem, p32, q5,
-                               (float)RKA[1], (float)RKB[0], s->status, s->stream, 1, s->kernel);
+                               (float)RKA[1], (float)RKB[0], s->status, s->stream, 1, s->kernel, 0);
   }
   if (e == cudaErrorNotSupported)  // returned by the launcher, not by CUDA
     return solver_fail(CB_ERR_UNSUPPORTED, "cb_solver_test_timeout: this shape does not run the pipelined stage");

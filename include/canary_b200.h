@@ -234,6 +234,28 @@ int cb_solver_current(const cb_solver *s, void **state);
 int cb_solver_settle(cb_solver *s);
 int cb_solver_pack(cb_solver *s, int what, const int64_t *elems, int64_t n, void *buf);
 int cb_solver_unpack(cb_solver *s, int what, const void *buf, int64_t first, int64_t n);
+/* Face-trace exchange: the minimal message of the partitioned solve.  A
+ * stage reads a ghost element only at the face nodes of the faces its own
+ * elements touch, so a neighbour needs Nfp·nstate values per shared face
+ * (Nfp·nstate·dim for the gradient) instead of whole elements.  codes
+ * (device int64, n entries) are (element << 3) | face: own elements
+ * 0 .. nelem-1 for pack, ghost slots 0 .. nghost-1 for unpack; buf holds
+ * n x components x Nfp values in the solver's precision (component-major
+ * per entry).  Entries out of range are skipped and raise CB_ERR_MESH in the
+ * status.  Stream-ordered on the solver's stream. */
+int cb_solver_pack_faces(cb_solver *s, int what, const int64_t *codes, int64_t n, void *buf);
+int cb_solver_unpack_faces(cb_solver *s, int what, const int64_t *codes, int64_t n, void *buf);
+/* Overlap of the ghost exchange with interior work (the reference runs
+ * volumerhs! while MPI receives are in flight, euler2d_set2c.jl:707-731):
+ * elements 0 .. ninterior-1 must read no ghost (the caller orders its own
+ * elements interior first).  cb_solver_stage_split(half = 0) runs the
+ * stage for those elements, half = 1 for the others (once the ghosts of the
+ * state the stage reads are filled) and then makes the other buffer
+ * current; a stage split this way equals cb_solver_stage bit for bit.
+ * Inviscid form, shapes whose stage runs over element ranges (the pipelined
+ * and tensor-core stages); CB_ERR_UNSUPPORTED otherwise. */
+int cb_solver_set_split(cb_solver *s, int64_t ninterior);
+int cb_solver_stage_split(cb_solver *s, int stage, double dt, int half, void **next_in);
 
 /* ---------------------------------------------------------------------- */
 /* Device-side geometry.                                                   */

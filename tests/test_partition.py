@@ -1,8 +1,10 @@
 """Element-partitioned solve (cb_solver_create_ghosted and the stage API):
 several parts of one mesh advanced in lock step in this process, ghosts moved
-by device copies, give the unpartitioned single-mesh result bit for bit —
-every element's arithmetic is the same.  The inter-rank transport is
-covered on the host (tests/test_partition_host.py, gloo)."""
+by device copies — face traces (the minimal message) or whole elements —
+with each inviscid stage split into its interior and boundary halves, give
+the unpartitioned single-mesh result bit for bit: every element's arithmetic
+is the same.  The inter-rank transport is covered on the host
+(tests/test_partition_host.py, gloo)."""
 import math
 
 import numpy as np
@@ -40,7 +42,8 @@ def square(N, n):
 @pytest.mark.parametrize("case,world,visc", [("cube3", 2, 0.0), ("cube3", 5, 0.0), ("cube4w", 3, 0.0),
                                              ("square", 4, 0.0), ("cube3", 3, 0.02), ("square", 2, 0.02)])
 @pytest.mark.parametrize("precision", [64, 32])
-def test_parts_equal_single_mesh(case, world, visc, precision):
+@pytest.mark.parametrize("faces", [True, False])
+def test_parts_equal_single_mesh(case, world, visc, precision, faces):
     """Inviscid and LDG Navier–Stokes (state and gradient exchanged)."""
     import torch
     m, Q, dt = {"cube3": lambda: cube(3, 4), "cube4w": lambda: cube(4, 3, walls=True),
@@ -54,10 +57,23 @@ def test_parts_equal_single_mesh(case, world, visc, precision):
     stream = torch.cuda.Stream()
     parts = [P.GhostedLSRK(m, P.plan(m, r, world), Q, precision, dg.make_phys(**phys), stream=stream)
              for r in range(world)]
-    P.run_parts(parts, k, dt)
+    if visc == 0.0:
+        assert all(p.split for p in parts)  # interior / boundary halves
+    P.run_parts(parts, k, dt, faces=faces)
     got = np.concatenate([p.state() for p in parts], axis=2)
     for p in parts:
         p.close()
     assert np.array_equal(got, ref)
-    if precision == 64:
+    if precision == 64 and faces:
         assert max(relerr_fields(got, oracle_run(m, Q, dt, k, phys=phys))) < 1e-12
+
+
+def test_face_traces_are_the_minimal_message():
+    """The trace exchange moves Nfp values per shared face and field; whole
+    elements move Np per element."""
+    m, Q, dt = cube(3, 4)
+    p = P.plan(m, 0, 2)
+    nfaces = sum(len(c) for _, c in p.recv_faces)
+    trace_values = nfaces * 16 * 5
+    element_values = sum(n for _, _, n in p.recv) * 64 * 5
+    assert trace_values < element_values / 3
