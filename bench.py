@@ -366,8 +366,15 @@ def batched_ensemble(count=512, seed=0, steps=500, device="cuda", parity_sample=
     shapes = sorted({(2, p["N"]) for p in params})
     for prec in (64, 32):
         t1 = time.time()
-        tuning = B.autotune(prec, shapes)  # stage variant per (dim, N), timed on this GPU
+        # stage variant per (dim, N), timed on this GPU on the ensemble's own
+        # instances of each shape (its size mix)
+        rep = {}
+        tuning = B.autotune(prec, shapes, instances=[(2, p["N"], p["n_side"]) for p in params], report=rep)
         out[f"autotune_fp{prec}_s"] = round(time.time() - t1, 2)
+        out[f"autotune_fp{prec}"] = {f"{d},{n}": {"variant": r["variant"], **r["config"],
+                                                   "instances": r["instances"], "nodes": r["nodes"],
+                                                   "ms_per_step": {str(v): round(t, 4) for v, t in r["ms_per_step"].items()}}
+                                     for (d, n), r in rep.items()}
         ens = B.VortexEnsemble(params, prec, nsteps=steps, cache=cache, tuning=tuning)
         torch.cuda.synchronize()
         ens.run(1)  # builds the step graph

@@ -22,10 +22,12 @@ MAX_ORDER = {2: 8, 3: 7}  # orders compiled into the batched stage
 # stage variants of one (dim, N): 0 = pipelined bulk-copy staging (where the
 # slabs are 16-byte multiples), 1 / 2 = grouped stage with ~256 / ~512 nodes
 # per block, 3 / 4 = pipelined staging compiled for 3 / 4 resident blocks per
-# SM (blocks of up to 256 threads)
-VARIANTS = (0, 1, 2, 3, 4)
-PIPELINED = (0, 3, 4)
+# SM (blocks of up to 256 threads), 6 = pipelined staging with copies two
+# element groups ahead
+VARIANTS = (0, 1, 2, 3, 4, 6)
+PIPELINED = (0, 3, 4, 6)
 VAR_AFFINE = 5  # the pipelined stage with affine-element geometry (chosen by the batch)
+VAR_DEEP = 6
 
 
 class BatchMesh:
@@ -86,6 +88,15 @@ class Batch:
         v = C.c_int(-1)
         check(_lib.lib().cb_batch_get_variant(self._h, dim, N, C.byref(v)))
         return v.value
+
+    def variant_info(self, dim: int, N: int, variant: int) -> dict:
+        """Launch configuration of a stage variant: elements per CTA, threads
+        per CTA, nodes per thread, element groups staged ahead (0: grouped
+        staging), resident CTAs per SM, shared memory per CTA."""
+        a = (C.c_int64 * 6)()
+        check(_lib.lib().cb_batch_variant_info(self._h, dim, N, variant, a))
+        return {"elements_per_cta": a[0], "threads_per_cta": a[1], "nodes_per_thread": a[2],
+                "staging_depth": a[3], "ctas_per_sm": a[4], "smem_per_cta": a[5]}
 
     def set_variant(self, dim: int, N: int, variant: int) -> None:
         """Stage variant for instances of (dim, N) admitted from now on
@@ -271,16 +282,93 @@ class VortexEnsemble:
 
 
 # ------------------------------------------------------------------ autotuner
+def _time_variants(precision, dim, N, meshes, steps, repeat):
+    """Step time of each stage variant of (dim, N) on the given instances
+    (pairs of a BatchMesh and a device state factory), all admitted to one
+    batch; {variant: ms per step} over the variants built for the shape."""
+    torch = _torch()
+    timings = {}
+    for var in VARIANTS:
+        b = Batch(precision, max(len(meshes), 1))
+        try:
+            b.set_variant(dim, N, var)
+        except Exception:
+            b.close()
+            continue
+        b.set_affine(False)  # time the variant itself
+        slots = []
+        for bm, make, dt in meshes:
+            Q = make()
+            slots.append(b.add(bm, Q, torch.zeros_like(Q), dt, 10 ** 9))
+        b.run(1)  # build the graph, warm up
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ts = []
+        for _ in range(repeat):
+            torch.cuda.synchronize()
+            ev0.record()
+            b.run(steps)
+            ev1.record()
+            torch.cuda.synchronize()
+            ts.append(ev0.elapsed_time(ev1) / steps)
+        timings[var] = min(ts)
+        for s in slots:
+            b.release(s)
+        b.close()
+    return timings
+
+
 def autotune(precision: int, shapes, nodes_target: int = 4_000_000, steps: int = 4, repeat: int = 3,
-             stream=None) -> dict:
-    """Choose the stage variant (pipelined staging at one of several
-    occupancies, or grouped with about 256 / 512 nodes per block) of each
-    (dim, N) by timing the batched step on a synthetic instance of that shape
-    with about `nodes_target` nodes: the 2-D vortex / the 3-D Fourier state
-    on periodic meshes built on the device.  Returns {(dim, N): variant}."""
+             stream=None, instances=None, report=None) -> dict:
+    """Choose the stage variant of each (dim, N) — pipelined staging at one of
+    several occupancies or two element groups ahead, or grouped staging with
+    about 256 / 512 nodes per block, i.e. elements per CTA, threads and nodes
+    per thread, and staging depth — by timing the batched step.
+
+    With `instances` (the workload's (dim, N, n_side) list) each shape is
+    timed on the workload's own instances of that shape, taken in order up to
+    about `nodes_target` nodes (its actual size mix); otherwise on one
+    synthetic instance of about `nodes_target` nodes: the 2-D vortex / the
+    3-D Fourier state on periodic meshes built on the device.  Returns
+    {(dim, N): variant}; `report` (a dict) receives, per shape, the timings
+    and the chosen variant's launch configuration."""
     torch = _torch()
     from . import ic
     best = {}
+    if instances is not None:
+        for dim, N in shapes:
+            L = 10.0 if dim == 2 else 2 * np.pi
+            picks, nodes = [], 0
+            for d, n, ns in instances:
+                if (d, n) == (dim, N) and nodes < nodes_target:
+                    picks.append(ns)
+                    nodes += ns ** dim * (N + 1) ** dim
+            dms = {}
+            meshes = []
+            real = torch.float64 if precision == 64 else torch.float32
+            for ns in picks:
+                if ns not in dms:
+                    dm = DeviceMesh.build(dim, N, (np.linspace(0.0, L, ns + 1),) * dim, (True,) * dim)
+                    dms[ns] = (dm, BatchMesh(dm, precision))
+                dm, bm = dms[ns]
+                X = dm.coords()
+                if dim == 2:
+                    make = (lambda X=X: ic.device_state(list(ic.isentropic_vortex_t(X[0], X[1], 5.0, 5.0, 5.0)), real))
+                    dt = 1e-4
+                else:
+                    make = (lambda X=X: ic.device_state(list(ic.fourier_state_t(X[0], X[1], X[2], seed=0)), real))
+                    dt = 1e-5
+                meshes.append((bm, make, dt))
+            timings = _time_variants(precision, dim, N, meshes, steps, repeat)
+            for dm, bm in dms.values():
+                bm.close()
+            best[(dim, N)] = min(timings, key=timings.get)
+            if report is not None:
+                info = Batch(precision, 1)
+                report[(dim, N)] = {"variant": best[(dim, N)], "instances": len(picks), "nodes": nodes,
+                                    "ms_per_step": timings,
+                                    "config": info.variant_info(dim, N, best[(dim, N)])}
+                info.close()
+        return best
     for dim, N in shapes:
         Np = (N + 1) ** dim
         n_side = max(2, int(round((nodes_target / Np) ** (1.0 / dim))))

@@ -189,7 +189,8 @@ BKernels<T> &b_kernels() {
 }
 template <typename T>
 bool b_var_ok(int dim, int N, int var) {
-  return b_order_ok(dim, N) && var >= 0 && var < NVAR_SEL && b_kernels<T>().fn[shape_id(dim, N, var)] != nullptr;
+  return b_order_ok(dim, N) && var >= 0 && var < NVAR && var != VAR_AFFINE &&
+         b_kernels<T>().fn[shape_id(dim, N, var)] != nullptr;
 }
 // viscous batches run the grouped two-pass LDG stage (variant 1 shapes)
 constexpr int VAR_VISC = 1;
@@ -796,6 +797,35 @@ int cb_batch_get_variant(const cb_batch *b, int dim, int N, int *variant) {
     return solver_fail(CB_ERR_ARG, "cb_batch_get_variant: bad arguments");
   *variant = b->var[dim - 2][N];
   return CB_OK;
+}
+
+}  // extern "C"
+
+namespace {
+template <typename T>
+int variant_info(int dim, int N, int variant, int64_t *info) {
+  const int sid = shape_id(dim, N, variant);
+  BKernels<T> &k = b_kernels<T>();
+  if (!k.fn[sid]) return solver_fail(CB_ERR_UNSUPPORTED, "cb_batch_variant_info: variant %d is not built", variant);
+  const cudaError_t e = b_prepare<T>(sid);
+  if (e != cudaSuccess) return solver_fail(CB_ERR_CUDA, "cb_batch_variant_info: %s", cudaGetErrorString(e));
+  const int Nq = N + 1, Np = dim == 2 ? Nq * Nq : Nq * Nq * Nq;
+  info[0] = k.epb[sid];
+  info[1] = k.threads[sid];
+  info[2] = ((int64_t)k.epb[sid] * Np + k.threads[sid] - 1) / k.threads[sid];
+  info[3] = k.ahead[sid];
+  info[4] = k.grid[sid] / num_sms();
+  info[5] = (int64_t)k.smem[sid];
+  return CB_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int cb_batch_variant_info(const cb_batch *b, int dim, int N, int variant, int64_t *info) {
+  if (!b || !info || (dim != 2 && dim != 3) || !b_order_ok(dim, N) || variant < 0 || variant >= NVAR)
+    return solver_fail(CB_ERR_ARG, "cb_batch_variant_info: bad arguments");
+  return b->prec == 64 ? variant_info<double>(dim, N, variant, info) : variant_info<float>(dim, N, variant, info);
 }
 
 int cb_batch_add(cb_batch *b, const cb_mesh *m, void *Q, void *rhs, double dt, int64_t nsteps, const double *qref,

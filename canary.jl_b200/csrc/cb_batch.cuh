@@ -59,11 +59,12 @@ struct alignas(16) BWork {
 // Shape id of (dim, N, variant); ids of shapes that are not built stay
 // unused.
 // Stage variants per (dim, N): 0 pipelined (default occupancy), 1 / 2
-// grouped (~256 / ~512 nodes), 3 / 4 pipelined at other occupancies — the
-// ones a caller may select — and VAR_AFFINE, the pipelined stage with
-// affine-element geometry, which the batch uses in place of a pipelined
-// variant for meshes whose elements are all affine (gravity off).
-constexpr int NVAR_SEL = 5, VAR_AFFINE = 5, NVAR = 6;
+// grouped (~256 / ~512 nodes), 3 / 4 pipelined at other occupancies,
+// VAR_DEEP pipelined with copies two groups ahead — the ones a caller may
+// select — and VAR_AFFINE, the pipelined stage with affine-element geometry,
+// which the batch uses in place of a pipelined variant for meshes whose
+// elements are all affine (gravity off).
+constexpr int VAR_AFFINE = 5, VAR_DEEP = 6, NVAR = 7;
 constexpr int NSHAPE = 2 * NVAR * (BMAXN2 + 1);
 __host__ __device__ constexpr int shape_id(int dim, int N, int var) {
   return (dim - 2) * NVAR * (BMAXN2 + 1) + NVAR * N + var;
@@ -732,6 +733,7 @@ template <typename T>
 struct BKernels {
   const void *fn[NSHAPE] = {};
   int epb[NSHAPE] = {}, threads[NSHAPE] = {}, grid[NSHAPE] = {};
+  int ahead[NSHAPE] = {};  // element groups whose copies are in flight ahead of the work (0: grouped)
   size_t smem[NSHAPE] = {};
   bool pipelined[NSHAPE] = {}, ready[NSHAPE] = {};
   // viscous batches (variant 1 shapes only): gradient and stage passes
@@ -755,6 +757,7 @@ void b_fill_pipe(BKernels<T> &k, int var) {
   k.threads[id] = Cfg<DIM, Nq>::THREADS;
   k.smem[id] = Pipe2<DIM, Nq, T, AFF, DEEP>::smem() + Src::RING_BYTES;
   k.pipelined[id] = true;
+  k.ahead[id] = DEEP ? 2 : 1;
 }
 template <int DIM, int Nq, typename T>
 void b_fill(BKernels<T> &k) {
@@ -767,6 +770,10 @@ void b_fill(BKernels<T> &k) {
       b_fill_pipe<DIM, Nq, T, M0 == 3 ? 2 : 3>(k, 3);
       b_fill_pipe<DIM, Nq, T, M0 == 4 ? 2 : 4>(k, 4);
     }
+    // the per-node stage with copies two groups ahead (staging depth 2), at
+    // the default occupancy where that fits
+    using PN = Pipe2<DIM, Nq, T, false, true>;
+    if constexpr (PN::OK && PN::fits(M0)) b_fill_pipe<DIM, Nq, T, M0, false, true>(k, VAR_DEEP);
     // the affine stage copies two groups ahead where that fits M0 blocks per SM
     using PD = Pipe2<DIM, Nq, T, true, true>;
     if constexpr (PD::OK && PD::fits(M0)) b_fill_pipe<DIM, Nq, T, M0, true, true>(k, VAR_AFFINE);

@@ -342,12 +342,19 @@ int cb_batch_create(cb_batch **out, int precision, int max_instances,
  * 0 = pipelined bulk-copy staging at its default occupancy (where every slab
  * is a multiple of 16 bytes: all 2-D orders, 3-D odd orders), 1 / 2 = grouped
  * staging with about 256 / 512 nodes per block, 3 / 4 = pipelined staging
- * compiled for the other occupancies (2, 3 or 4 blocks per SM).  Variants
+ * compiled for the other occupancies (2, 3 or 4 blocks per SM), 6 = pipelined
+ * staging with copies two element groups ahead instead of one.  Variants
  * that are not built for (dim, N) give CB_ERR_UNSUPPORTED.  Chosen by an
  * autotuner; the pipelined variants agree bit for bit among themselves, as do
  * the grouped ones, and the two families to round-off. */
 int cb_batch_set_variant(cb_batch *b, int dim, int N, int variant);
 int cb_batch_get_variant(const cb_batch *b, int dim, int N, int *variant);
+/* Launch configuration of a stage variant of (dim, N) in this batch's
+ * precision (5: the affine-element stage): info[0] elements per CTA,
+ * info[1] threads per CTA, info[2] nodes per thread, info[3] element groups
+ * staged ahead of the work (0: grouped staging, no copies in flight),
+ * info[4] resident CTAs per SM, info[5] dynamic shared memory per CTA. */
+int cb_batch_variant_info(const cb_batch *b, int dim, int N, int variant, int64_t *info);
 /* Instances admitted from now on whose mesh is affine (cb_mesh_affine), with
  * gravity 0 and a pipelined variant selected, use the affine-element stage
  * when `on`; it reads no vgeo / sgeo and uses each element's first-node

@@ -91,9 +91,9 @@ def test_batch_result_same_alone_and_in_mix(cases, precision):
 @pytest.mark.parametrize("precision", [64, 32])
 def test_batch_variants_agree(cases, precision):
     """Grouped variants (1, 2) are bit-identical to each other, and so are the
-    pipelined ones (0, 3, 4: the same code at other occupancies); the two
-    families sum the contraction differently (padded rows) and agree to
-    round-off."""
+    pipelined ones (0, 3, 4, 6: the same code at other occupancies or staging
+    depth); the two families sum the contraction differently (padded rows)
+    and agree to round-off."""
     orders = [(m.dim, m.N) for (m, Q, dt, k) in cases]
     probe = B.Batch(precision, 1)
     built = {}
@@ -113,7 +113,7 @@ def test_batch_variants_agree(cases, precision):
         if built[(m.dim, m.N, 2)]:
             assert np.array_equal(runs[1][i], runs[2][i])
         if built[(m.dim, m.N, 0)]:
-            for v in (3, 4):
+            for v in (3, 4, 6):
                 if built[(m.dim, m.N, v)]:
                     assert np.array_equal(runs[0][i], runs[v][i])
         assert max(relerr_fields(runs[0][i], runs[1][i])) < tol
@@ -215,6 +215,26 @@ def test_autotuner_picks_a_built_variant():
         assert b.variant(dim, N) == v
     b.close()
     assert (3, 4) in tuned and tuned[(3, 4)] in B.VARIANTS
+
+
+def test_autotuner_on_the_workload_size_mix_reports_the_configuration():
+    """Tuning on the workload's own instances of each shape (several mesh
+    sizes) reports the chosen variant's elements per CTA, threads, nodes per
+    thread, staging depth and CTAs per SM."""
+    inst = [(2, 4, 6), (2, 4, 10), (2, 6, 4), (2, 4, 8), (2, 6, 12)]
+    rep = {}
+    tuned = B.autotune(32, [(2, 4), (2, 6)], nodes_target=50000, steps=1, repeat=1, instances=inst, report=rep)
+    assert set(tuned) == {(2, 4), (2, 6)}
+    assert rep[(2, 4)]["instances"] == 3 and rep[(2, 6)]["instances"] == 2
+    for key, r in rep.items():
+        c = r["config"]
+        assert r["variant"] == tuned[key] and r["variant"] in r["ms_per_step"]
+        assert c["threads_per_cta"] >= 32 and c["elements_per_cta"] >= 1 and c["ctas_per_sm"] >= 1
+        assert c["nodes_per_thread"] >= 1 and c["staging_depth"] in (0, 1, 2)
+    b = B.Batch(32, 1)
+    assert b.variant_info(2, 4, B.VAR_DEEP)["staging_depth"] == 2
+    assert b.variant_info(2, 4, 0)["staging_depth"] == 1 and b.variant_info(2, 4, 1)["staging_depth"] == 0
+    b.close()
 
 
 def test_invalid_mesh_is_reported_at_first_use(cases):
