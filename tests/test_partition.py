@@ -40,14 +40,15 @@ def square(N, n):
 
 
 @pytest.mark.parametrize("case,world,visc", [("cube3", 2, 0.0), ("cube3", 5, 0.0), ("cube4w", 3, 0.0),
-                                             ("square", 4, 0.0), ("cube3", 3, 0.02), ("square", 2, 0.02)])
+                                             ("square", 4, 0.0), ("cube3", 3, 0.02), ("square", 2, 0.02),
+                                             ("cube7", 2, 0.0)])
 @pytest.mark.parametrize("precision", [64, 32])
 @pytest.mark.parametrize("faces", [True, False])
 def test_parts_equal_single_mesh(case, world, visc, precision, faces):
     """Inviscid and LDG Navier–Stokes (state and gradient exchanged)."""
     import torch
     m, Q, dt = {"cube3": lambda: cube(3, 4), "cube4w": lambda: cube(4, 3, walls=True),
-                "square": lambda: square(5, 6)}[case]()
+                "square": lambda: square(5, 6), "cube7": lambda: cube(7, 3)}[case]()
     k = 3
     phys = dict(dg.WORKLOAD_PHYS, visc=visc)
     single = dg.LSRK.for_state(dg.DeviceMesh.upload(m), Q, precision, phys=dg.make_phys(**phys))
