@@ -344,7 +344,8 @@ def ensemble_parity(params, cache, finals, sample=16, steps=500, dt=0.002, threa
             "oracle_seconds": time.perf_counter() - t0}
 
 
-def batched_ensemble(count=512, seed=0, steps=500, device="cuda", parity_sample=16):
+def batched_ensemble(count=512, seed=0, steps=500, device="cuda", parity_sample=16, precisions=(64, 32),
+                     tune=True):
     """The batched workload: `count` independent 2-D vortex instances (N, mesh,
     strength and centre drawn per instance from PCG64(seed + i)), dt = 0.002,
     `steps` LSRK(5,4) steps each, advanced together by one Batch per precision
@@ -364,12 +365,13 @@ def batched_ensemble(count=512, seed=0, steps=500, device="cuda", parity_sample=
            "host_mesh_setup_s": round(time.time() - t0, 2)}
     finals = {}
     shapes = sorted({(2, p["N"]) for p in params})
-    for prec in (64, 32):
+    for prec in precisions:
         t1 = time.time()
         # stage variant per (dim, N), timed on this GPU on the ensemble's own
-        # instances of each shape (its size mix)
+        # instances of each shape (its size mix); the batch's defaults without it
         rep = {}
-        tuning = B.autotune(prec, shapes, instances=[(2, p["N"], p["n_side"]) for p in params], report=rep)
+        tuning = B.autotune(prec, shapes, instances=[(2, p["N"], p["n_side"]) for p in params],
+                            report=rep) if tune else {}
         out[f"autotune_fp{prec}_s"] = round(time.time() - t1, 2)
         out[f"autotune_fp{prec}"] = {f"{d},{n}": {"variant": r["variant"], **r["config"],
                                                    "instances": r["instances"], "nodes": r["nodes"],
@@ -414,13 +416,14 @@ def batched_ensemble(count=512, seed=0, steps=500, device="cuda", parity_sample=
                                          "kernel": "k_stage_pipe2 (one persistent kernel per shape, "
                                                    "five stage launches per step)"}}
         ens.close()
-    err = np.zeros(4)
-    for a, b in zip(finals[32], finals[64]):
-        for q in range(4):
-            err[q] = max(err[q], np.linalg.norm(a[:, q] - b[:, q]) / np.linalg.norm(b[:, q]))
-    out["fp32_rel_l2_vs_fp64_max_over_instances"] = {"U": err[0], "V": err[1], "rho": err[2], "E": err[3]}
-    if parity_sample:
-        out["parity_vs_oracle"] = ensemble_parity(params, cache, finals, parity_sample, steps)
+    if 32 in finals and 64 in finals:
+        err = np.zeros(4)
+        for a, b in zip(finals[32], finals[64]):
+            for q in range(4):
+                err[q] = max(err[q], np.linalg.norm(a[:, q] - b[:, q]) / np.linalg.norm(b[:, q]))
+        out["fp32_rel_l2_vs_fp64_max_over_instances"] = {"U": err[0], "V": err[1], "rho": err[2], "E": err[3]}
+        if parity_sample:
+            out["parity_vs_oracle"] = ensemble_parity(params, cache, finals, parity_sample, steps)
     cache.close()
     return out
 
@@ -521,6 +524,10 @@ def main():
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched-ensemble measurement (run on 1 GPU only)")
     ap.add_argument("--batched-instances", type=int, default=512)
+    ap.add_argument("--batched-steps", type=int, default=500)
+    ap.add_argument("--batched-precisions", type=int, nargs="+", default=[64, 32], choices=[64, 32])
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="batched section: the batch's default stage variants instead of the autotuner's")
     ap.add_argument("--no-served", action="store_true",
                     help="skip the served-stream measurement (run on 1 GPU only)")
     ap.add_argument("--served-requests", type=int, default=150)
@@ -684,9 +691,10 @@ def main():
     elif rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_sample(N, args.cpu_seconds)
     if world == 1 and not args.no_batched:
-        bat = batched_ensemble(args.batched_instances, device=dev,
-                               parity_sample=16 if args.parity_steps > 0 else 0)
-        if args.precision == 64:
+        bat = batched_ensemble(args.batched_instances, steps=args.batched_steps, device=dev,
+                               parity_sample=16 if args.parity_steps > 0 else 0,
+                               precisions=tuple(args.batched_precisions), tune=not args.no_autotune)
+        if args.precision == 64 and "fp32" in bat:
             bat["fp32_over_fp64_plain"] = bat["fp32"]["value"] / value
         line["batched"] = bat
     if world == 1 and not args.no_served:

@@ -23,11 +23,13 @@ MAX_ORDER = {2: 8, 3: 7}  # orders compiled into the batched stage
 # slabs are 16-byte multiples), 1 / 2 = grouped stage with ~256 / ~512 nodes
 # per block, 3 / 4 = pipelined staging compiled for 3 / 4 resident blocks per
 # SM (blocks of up to 256 threads), 6 = pipelined staging with copies two
-# element groups ahead
-VARIANTS = (0, 1, 2, 3, 4, 6)
-PIPELINED = (0, 3, 4, 6)
+# element groups ahead, 7 = pipelined staging with twice the elements per
+# group on 512-thread blocks
+VARIANTS = (0, 1, 2, 3, 4, 6, 7)
+PIPELINED = (0, 3, 4, 6, 7)
 VAR_AFFINE = 5  # the pipelined stage with affine-element geometry (chosen by the batch)
 VAR_DEEP = 6
+VAR_WIDE = 7
 
 
 class BatchMesh:

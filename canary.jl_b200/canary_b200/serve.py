@@ -204,8 +204,9 @@ class _Live:
 
 
 def _pcts(lat):
+    # no completed request: the statistics are undefined (None, JSON null)
     if not len(lat):
-        return {"p50_s": float("nan"), "p99_s": float("nan"), "mean_s": float("nan")}
+        return {"p50_s": None, "p99_s": None, "mean_s": None}
     a = np.asarray(lat)
     return {"p50_s": float(np.percentile(a, 50)), "p99_s": float(np.percentile(a, 99)), "mean_s": float(a.mean())}
 
@@ -238,10 +239,10 @@ class Report:
         out = {"requests": len(self.kinds) or len(self.latencies), "completed": len(done),
                "failed": len(self.failed), "rejected": len(self.rejected), "cancelled": len(self.cancelled)}
         out.update(_pcts(list(done.values())))
-        out.update({"solves_per_s": len(done) / span if ok else float("nan"), "span_s": span,
-                    "dof_stage_per_s": self.dof_stage / span if ok else float("nan"),
+        out.update({"solves_per_s": len(done) / span if ok else None, "span_s": span,
+                    "dof_stage_per_s": self.dof_stage / span if ok else None,
                     "completed_dof_stage_per_s":
-                        sum(self.work.get(r, 0.0) for r in done) / span if ok else float("nan"),
+                        sum(self.work.get(r, 0.0) for r in done) / span if ok else None,
                     "peak_hbm_bytes": self.peak_bytes, "max_concurrent": self.max_live})
         if self.kinds:
             per = {}
@@ -636,7 +637,7 @@ def benchmark(count=2000, seed=0, precision=32, hbm_budget=120e9, tick_steps=8, 
         srv = Server(precision, hbm_budget, tick_steps=tick_steps, device=device)
         cap = srv.serve(cap_reqs, realtime=False).summary()
         srv.close()
-        rate = load * cap["solves_per_s"]  # completed solves only
+        rate = load * (cap["solves_per_s"] or 0.0)  # completed solves only (0: all arrive at once)
         reqs = request_stream(count, rate, seed, vel_peak=vel_peak)
         srv = Server(precision, hbm_budget, tick_steps=tick_steps, device=device)
         served = srv.serve(reqs, realtime=True)

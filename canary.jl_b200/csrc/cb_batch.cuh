@@ -60,11 +60,12 @@ struct alignas(16) BWork {
 // unused.
 // Stage variants per (dim, N): 0 pipelined (default occupancy), 1 / 2
 // grouped (~256 / ~512 nodes), 3 / 4 pipelined at other occupancies,
-// VAR_DEEP pipelined with copies two groups ahead — the ones a caller may
+// VAR_DEEP pipelined with copies two groups ahead, VAR_WIDE pipelined with
+// twice the elements per group on 512-thread blocks — the ones a caller may
 // select — and VAR_AFFINE, the pipelined stage with affine-element geometry,
 // which the batch uses in place of a pipelined variant for meshes whose
 // elements are all affine (gravity off).
-constexpr int VAR_AFFINE = 5, VAR_DEEP = 6, NVAR = 7;
+constexpr int VAR_AFFINE = 5, VAR_DEEP = 6, VAR_WIDE = 7, NVAR = 8;
 constexpr int NSHAPE = 2 * NVAR * (BMAXN2 + 1);
 __host__ __device__ constexpr int shape_id(int dim, int N, int var) {
   return (dim - 2) * NVAR * (BMAXN2 + 1) + NVAR * N + var;
@@ -721,8 +722,8 @@ struct BatchSrc {
   __device__ T rkbdt(int it) const { return T(rkb * at(it).d.dt); }
   __device__ unsigned *status(int it) const { return at(it).d.status; }
 };
-template <int DIM, int Nq, typename T, int RING = 3>
-using BPipeSrc = BatchSrc<T, Lay<DIM>::NS, Cfg<DIM, Nq>::EPB, RING>;
+template <int DIM, int Nq, typename T, int RING = 3, int X = 1>
+using BPipeSrc = BatchSrc<T, Lay<DIM>::NS, CfgX<DIM, Nq, X>::EPB, RING>;
 
 inline bool b_order_ok(int dim, int N) { return N >= 1 && N <= (dim == 2 ? BMAXN2 : BMAXN3); }
 
@@ -748,14 +749,14 @@ constexpr size_t b_group_smem() {
   return sizeof(T) * (((Nq * Nq + 1) & ~1) + (size_t)Lay<DIM>::NS * C::SLOTS +
                       (size_t)DIM * Lay<DIM>::NS * C::SLOTS);
 }
-template <int DIM, int Nq, typename T, int MINB, bool AFF = false, bool DEEP = false>
+template <int DIM, int Nq, typename T, int MINB, bool AFF = false, bool DEEP = false, int X = 1>
 void b_fill_pipe(BKernels<T> &k, int var) {
-  using Src = BPipeSrc<DIM, Nq, T, DEEP ? 4 : 3>;
+  using Src = BPipeSrc<DIM, Nq, T, DEEP ? 4 : 3, X>;
   const int id = shape_id(DIM, Nq - 1, var);
-  k.fn[id] = (const void *)k_stage_pipe2<DIM, Nq, T, Src, MINB, AFF, DEEP>;
-  k.epb[id] = Cfg<DIM, Nq>::EPB;
-  k.threads[id] = Cfg<DIM, Nq>::THREADS;
-  k.smem[id] = Pipe2<DIM, Nq, T, AFF, DEEP>::smem() + Src::RING_BYTES;
+  k.fn[id] = (const void *)k_stage_pipe2<DIM, Nq, T, Src, MINB, AFF, DEEP, X>;
+  k.epb[id] = CfgX<DIM, Nq, X>::EPB;
+  k.threads[id] = CfgX<DIM, Nq, X>::THREADS;
+  k.smem[id] = Pipe2<DIM, Nq, T, AFF, DEEP, X>::smem() + Src::RING_BYTES;
   k.pipelined[id] = true;
   k.ahead[id] = DEEP ? 2 : 1;
 }
@@ -774,6 +775,11 @@ void b_fill(BKernels<T> &k) {
     // the default occupancy where that fits
     using PN = Pipe2<DIM, Nq, T, false, true>;
     if constexpr (PN::OK && PN::fits(M0)) b_fill_pipe<DIM, Nq, T, M0, false, true>(k, VAR_DEEP);
+    // twice the elements per group on twice the threads (blocks of 512)
+    if constexpr (Cfg<DIM, Nq>::THREADS <= 256) {
+      using PW = Pipe2<DIM, Nq, T, false, false, 2>;
+      if constexpr (PW::OK && PW::fits(PW::MINB)) b_fill_pipe<DIM, Nq, T, PW::MINB, false, false, 2>(k, VAR_WIDE);
+    }
     // the affine stage copies two groups ahead where that fits M0 blocks per SM
     using PD = Pipe2<DIM, Nq, T, true, true>;
     if constexpr (PD::OK && PD::fits(M0)) b_fill_pipe<DIM, Nq, T, M0, true, true>(k, VAR_AFFINE);

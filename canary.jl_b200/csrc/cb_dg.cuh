@@ -77,6 +77,20 @@ struct Cfg {
   static constexpr int FPT = cdiv(FSLOTS, THREADS);
 };
 
+// The same with X times the elements per group and X times the threads (the
+// same nodes per thread): larger groups share each block barrier among more
+// nodes.  X = 1 is Cfg.
+template <int DIM, int Nq, int X>
+struct CfgX : Cfg<DIM, Nq> {
+  using B = Cfg<DIM, Nq>;
+  static constexpr int EPB = B::EPB * X;
+  static constexpr int SLOTS = EPB * B::Np;
+  static constexpr int THREADS = B::THREADS * X;
+  static constexpr int NPT = cdiv(SLOTS, THREADS);
+  static constexpr int FSLOTS = EPB * B::NFACE * B::Nfp;
+  static constexpr int FPT = cdiv(FSLOTS, THREADS);
+};
+
 // ---------------------------------------------------------------- physics
 template <int DIM, typename T>
 __device__ __forceinline__ T pressure(const T *q, T gc, const PhysT<T> &p) {

@@ -102,10 +102,11 @@ __host__ __device__ constexpr int row_stride(int nq) {
   return ((rs / vw) % 2 == 1) ? rs : rs + vw;
 }
 
-// Shared-memory plan of the pipelined stage for one (dim, Nq, T).
-template <int DIM, int Nq, typename T>
+// Shared-memory plan of the pipelined stage for one (dim, Nq, T) and X times
+// the elements per group of Cfg.
+template <int DIM, int Nq, typename T, int X = 1>
 struct Pipe {
-  using C = Cfg<DIM, Nq>;
+  using C = CfgX<DIM, Nq, X>;
   static constexpr int NS = Lay<DIM>::NS;
   static constexpr int NG = DIM * DIM + 2;  // staged vgeo fields: metric, MJ, MJI
   static constexpr int VW = 16 / (int)sizeof(T);   // elements per 16-byte vector
@@ -158,10 +159,10 @@ __device__ __forceinline__ void load_row(const T *src, T *dst) {
 
 // Tensor-product contraction of one node from direction-major flux rows:
 // R[s] += Σ_m D[m,i] Fξ[m;j,k] (then η, then ζ), each sum in m order.
-template <int DIM, int Nq, typename T>
+template <int DIM, int Nq, typename T, int X = 1>
 __device__ __forceinline__ void contract_rows(const T *flux, const T *DT, int el, int n, T *R) {
-  using PP = Pipe<DIM, Nq, T>;
-  constexpr int NS = Lay<DIM>::NS, MV = PP::MV, RS = PP::RS, NR = PP::NR, EPB = Cfg<DIM, Nq>::EPB;
+  using PP = Pipe<DIM, Nq, T, X>;
+  constexpr int NS = Lay<DIM>::NS, MV = PP::MV, RS = PP::RS, NR = PP::NR, EPB = CfgX<DIM, Nq, X>::EPB;
   const int i = n % Nq, j = (n / Nq) % Nq, k = DIM == 3 ? n / (Nq * Nq) : 0;
 #pragma unroll
   for (int r = 0; r < DIM; ++r) {

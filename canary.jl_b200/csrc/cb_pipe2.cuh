@@ -49,10 +49,13 @@ namespace cb {
 // group it + 2 is issued at the top of iteration it) — so that a block keeps
 // about twice the bytes in flight, for small groups whose copy latency a
 // single group of work does not cover.
-template <int DIM, int Nq, typename T, bool AFF = false, bool DEEP = false>
+//
+// X: X times the elements per group of Cfg, on X times the threads (the same
+// nodes per thread), so that each block barrier is shared by more nodes.
+template <int DIM, int Nq, typename T, bool AFF = false, bool DEEP = false, int X = 1>
 struct Pipe2 {
-  using C = Cfg<DIM, Nq>;
-  using P1 = Pipe<DIM, Nq, T>;
+  using C = CfgX<DIM, Nq, X>;
+  using P1 = Pipe<DIM, Nq, T, X>;
   static constexpr int NS = Lay<DIM>::NS, NSG = Lay<DIM>::NSG, NVG = Lay<DIM>::NVG;
   static constexpr int NG = P1::NG, RS = P1::RS, NR = P1::NR, MV = P1::MV;
   static constexpr size_t QB = P1::QB, GB = P1::GB;
@@ -89,7 +92,9 @@ struct Pipe2 {
   static constexpr size_t RING_MAX = 640;
   static constexpr bool OK = BULK && smem() + RING_MAX <= SMEM_LIMIT;
   // blocks of up to 256 threads are sized for two (FP64) or four (FP32) per SM
-  static constexpr int MINB = C::THREADS <= 256 ? (sizeof(T) == 4 ? 4 : 2) : 1;
+  // (larger groups of X > 1: 512-thread FP32 blocks two per SM)
+  static constexpr int MINB =
+      C::THREADS <= 256 ? (sizeof(T) == 4 ? 4 : 2) : (X > 1 && C::THREADS <= 512 && sizeof(T) == 4 ? 2 : 1);
   // whether `blocks` blocks fit in one SM's shared memory (228 KB, 1 KB of
   // it reserved per block)
   static constexpr bool fits(int blocks) { return blocks * (smem() + RING_MAX + 1024) <= 228 * 1024; }
@@ -147,13 +152,13 @@ struct MeshSrc {
 
 // MINB: resident blocks per SM that the register allocation is sized for;
 // AFF: affine-element geometry (see Pipe2; gravity must be zero); DEEP:
-// copies two groups ahead (see Pipe2).
+// copies two groups ahead (see Pipe2); X: X times the elements per group.
 template <int DIM, int Nq, typename T, typename Src, int MINB = Pipe2<DIM, Nq, T>::MINB, bool AFF = false,
-          bool DEEP = false>
-__global__ void __launch_bounds__(Cfg<DIM, Nq>::THREADS, MINB)
+          bool DEEP = false, int X = 1>
+__global__ void __launch_bounds__(CfgX<DIM, Nq, X>::THREADS, MINB)
 k_stage_pipe2(Src src, PhysT<T> p, T rka) {
-  using C = Cfg<DIM, Nq>;
-  using PP = Pipe2<DIM, Nq, T, AFF, DEEP>;
+  using C = CfgX<DIM, Nq, X>;
+  using PP = Pipe2<DIM, Nq, T, AFF, DEEP, X>;
   static_assert(Src::AHEAD >= PP::LOOK, "the source must publish the groups whose copies are issued");
   constexpr int NS = Lay<DIM>::NS, NVG = Lay<DIM>::NVG, NSG = Lay<DIM>::NSG, IR = Lay<DIM>::IR;
   constexpr int Np = C::Np, Nfp = C::Nfp, NF = C::NFACE, EPB = C::EPB, SP = C::SLOTS;
@@ -458,7 +463,7 @@ k_stage_pipe2(Src src, PhysT<T> p, T rka) {
 #pragma unroll
         for (int s = 0; s < NS; ++s) R[s] = Tc[(el * NS + s) * Np + n];
         R[DIM - 1] -= buoy[u];
-        contract_rows<DIM, Nq, T>(sF, DT, el, n, R);
+        contract_rows<DIM, Nq, T, X>(sF, DT, el, n, R);
         gather_face_terms<DIM, Nq, EPB, T>(FF, el, n, R);
 #pragma unroll
         for (int s = 0; s < NS; ++s) {

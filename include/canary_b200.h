@@ -343,7 +343,9 @@ int cb_batch_create(cb_batch **out, int precision, int max_instances,
  * is a multiple of 16 bytes: all 2-D orders, 3-D odd orders), 1 / 2 = grouped
  * staging with about 256 / 512 nodes per block, 3 / 4 = pipelined staging
  * compiled for the other occupancies (2, 3 or 4 blocks per SM), 6 = pipelined
- * staging with copies two element groups ahead instead of one.  Variants
+ * staging with copies two element groups ahead instead of one, 7 = pipelined
+ * staging with twice the elements per group on twice the threads (shapes
+ * whose default block has at most 256 threads).  Variants
  * that are not built for (dim, N) give CB_ERR_UNSUPPORTED.  Chosen by an
  * autotuner; the pipelined variants agree bit for bit among themselves, as do
  * the grouped ones, and the two families to round-off. */

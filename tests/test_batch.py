@@ -91,9 +91,9 @@ def test_batch_result_same_alone_and_in_mix(cases, precision):
 @pytest.mark.parametrize("precision", [64, 32])
 def test_batch_variants_agree(cases, precision):
     """Grouped variants (1, 2) are bit-identical to each other, and so are the
-    pipelined ones (0, 3, 4, 6: the same code at other occupancies or staging
-    depth); the two families sum the contraction differently (padded rows)
-    and agree to round-off."""
+    pipelined ones (0, 3, 4, 6, 7: the same code at other occupancies, staging
+    depth or group size); the two families sum the contraction differently
+    (padded rows) and agree to round-off."""
     orders = [(m.dim, m.N) for (m, Q, dt, k) in cases]
     probe = B.Batch(precision, 1)
     built = {}
@@ -113,7 +113,7 @@ def test_batch_variants_agree(cases, precision):
         if built[(m.dim, m.N, 2)]:
             assert np.array_equal(runs[1][i], runs[2][i])
         if built[(m.dim, m.N, 0)]:
-            for v in (3, 4, 6):
+            for v in (3, 4, 6, 7):
                 if built[(m.dim, m.N, v)]:
                     assert np.array_equal(runs[0][i], runs[v][i])
         assert max(relerr_fields(runs[0][i], runs[1][i])) < tol
@@ -232,7 +232,10 @@ def test_autotuner_on_the_workload_size_mix_reports_the_configuration():
         assert c["threads_per_cta"] >= 32 and c["elements_per_cta"] >= 1 and c["ctas_per_sm"] >= 1
         assert c["nodes_per_thread"] >= 1 and c["staging_depth"] in (0, 1, 2)
     b = B.Batch(32, 1)
-    assert b.variant_info(2, 4, B.VAR_DEEP)["staging_depth"] == 2
+    # copies two groups ahead are built where they fit four FP32 blocks per SM (2-D N >= 6)
+    assert b.variant_info(2, 6, B.VAR_DEEP)["staging_depth"] == 2
+    with pytest.raises(CanaryError):
+        b.variant_info(2, 4, B.VAR_DEEP)
     assert b.variant_info(2, 4, 0)["staging_depth"] == 1 and b.variant_info(2, 4, 1)["staging_depth"] == 0
     b.close()
 
