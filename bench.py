@@ -397,7 +397,7 @@ def batched_ensemble(count=512, seed=0, steps=500, device="cuda", parity_sample=
         for p, slot in zip(params, ens.slots):
             Np = (p["N"] + 1) ** 2
             nodes = Np * p["n_side"] ** 2
-            if ens.batch.slot_variant(slot) == B.VAR_AFFINE:
+            if ens.batch.slot_variant(slot) in B.AFFINE:
                 bpn = w * (4 * 4 + 17.0 / Np)  # state + carry, record of 17 values per element
             else:
                 bpn = bytes_per_node(2, p["N"], w)

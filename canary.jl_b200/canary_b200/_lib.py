@@ -31,7 +31,7 @@ EXPORTS = (
     "cb_solver_set_split", "cb_solver_stage_split",
     "cb_computegeometry", "cb_brickmesh", "cb_mesh_create", "cb_mesh_affine", "cb_mesh_destroy",
     "cb_batch_create", "cb_batch_set_variant", "cb_batch_get_variant", "cb_batch_set_affine",
-    "cb_batch_slot_variant", "cb_batch_variant_info", "cb_batch_add",
+    "cb_batch_set_concurrent", "cb_batch_slot_variant", "cb_batch_variant_info", "cb_batch_add",
     "cb_batch_run", "cb_batch_info", "cb_batch_release", "cb_batch_status", "cb_batch_status_async", "cb_batch_destroy",
 )
 
@@ -106,6 +106,7 @@ def lib() -> C.CDLL:
     L.cb_brickmesh.argtypes = [C.c_int, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp, vp]
     L.cb_mesh_affine.argtypes = [vp, C.POINTER(C.c_int)]
     L.cb_batch_set_affine.argtypes = [vp, C.c_int]
+    L.cb_batch_set_concurrent.argtypes = [vp, C.c_int]
     L.cb_batch_slot_variant.argtypes = [vp, C.c_int, C.POINTER(C.c_int)]
     L.cb_batch_variant_info.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.POINTER(i64)]
     L.cb_batch_create.argtypes = [C.POINTER(vp), C.c_int, C.c_int, phys_p, vp]

@@ -24,12 +24,19 @@ MAX_ORDER = {2: 8, 3: 7}  # orders compiled into the batched stage
 # per block, 3 / 4 = pipelined staging compiled for 3 / 4 resident blocks per
 # SM (blocks of up to 256 threads), 6 = pipelined staging with copies two
 # element groups ahead, 7 = pipelined staging with twice the elements per
-# group on 512-thread blocks
-VARIANTS = (0, 1, 2, 3, 4, 6, 7)
-PIPELINED = (0, 3, 4, 6, 7)
-VAR_AFFINE = 5  # the pipelined stage with affine-element geometry (chosen by the batch)
+# group on 512-thread blocks, 8 = pipelined staging with two nodes per thread;
+# 5 / 9 = the affine-element stage (copies two groups ahead) with one / two
+# nodes per thread, for meshes whose elements are all affine; 10 = the
+# tensor-core stage (3-D N = 7)
+VARIANTS = (0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10)
+PIPELINED = (0, 3, 4, 6, 7, 8)  # per-node geometry, bit-identical among themselves
+AFFINE = (5, 9)  # affine-element geometry, bit-identical among themselves
+VAR_AFFINE = 5
 VAR_DEEP = 6
 VAR_WIDE = 7
+VAR_NPT2 = 8
+VAR_AFFINE_NPT2 = 9
+VAR_MMA = 10
 
 
 class BatchMesh:
@@ -102,15 +109,26 @@ class Batch:
 
     def set_variant(self, dim: int, N: int, variant: int) -> None:
         """Stage variant for instances of (dim, N) admitted from now on
-        (VARIANTS); raises CanaryError for a variant not built for it."""
+        (VARIANTS); raises CanaryError for a variant not built for it.  A
+        chosen variant runs as chosen (an affine one only on meshes that
+        allow it, the shape's default per-node variant elsewhere); without a
+        choice the batch runs VAR_AFFINE where the affine stage applies."""
         check(_lib.lib().cb_batch_set_variant(self._h, dim, N, variant))
 
     def set_affine(self, on: bool) -> None:
-        """Whether instances admitted from now on use the affine-element stage
-        where it applies (affine mesh, gravity 0, pipelined variant; on by
-        default): it reads one geometry record per element instead of the
-        per-node metric and face geometry, and agrees with them to round-off."""
+        """Whether instances admitted from now on may use the affine-element
+        stage where it applies (affine mesh, gravity 0; on by default for
+        precision 32, off for 64): it reads one geometry record per element
+        instead of the per-node metric and face geometry, and agrees with
+        them to round-off."""
         check(_lib.lib().cb_batch_set_affine(self._h, 1 if on else 0))
+
+    def set_concurrent(self, on: bool) -> None:
+        """Step-graph order of the shapes present: True (default) = one chain
+        per shape, the chains concurrent; False = every RK stage of every
+        shape in turn, each stage kernel with the whole GPU.  Results do not
+        depend on it."""
+        check(_lib.lib().cb_batch_set_concurrent(self._h, 1 if on else 0))
 
     def add(self, mesh: BatchMesh, Q, rhs, dt: float, nsteps: int, qref=None) -> int:
         """Admit the caller's device state Q and zeroed carry rhs (flat tensors
@@ -284,20 +302,24 @@ class VortexEnsemble:
 
 
 # ------------------------------------------------------------------ autotuner
-def _time_variants(precision, dim, N, meshes, steps, repeat):
+def _time_variants(precision, dim, N, meshes, steps, repeat, affine):
     """Step time of each stage variant of (dim, N) on the given instances
     (pairs of a BatchMesh and a device state factory), all admitted to one
-    batch; {variant: ms per step} over the variants built for the shape."""
+    batch; {variant: ms per step} over the variants built for the shape (the
+    affine ones only when `affine`: every mesh affine and the affine stage
+    allowed)."""
     torch = _torch()
     timings = {}
     for var in VARIANTS:
+        if var in AFFINE and not affine:
+            continue
         b = Batch(precision, max(len(meshes), 1))
         try:
-            b.set_variant(dim, N, var)
+            b.set_variant(dim, N, var)  # a chosen variant runs as chosen
         except Exception:
             b.close()
             continue
-        b.set_affine(False)  # time the variant itself
+        b.set_affine(var in AFFINE)
         slots = []
         for bm, make, dt in meshes:
             Q = make()
@@ -320,11 +342,14 @@ def _time_variants(precision, dim, N, meshes, steps, repeat):
 
 
 def autotune(precision: int, shapes, nodes_target: int = 4_000_000, steps: int = 4, repeat: int = 3,
-             stream=None, instances=None, report=None) -> dict:
+             stream=None, instances=None, report=None, affine=None) -> dict:
     """Choose the stage variant of each (dim, N) — pipelined staging at one of
-    several occupancies or two element groups ahead, or grouped staging with
-    about 256 / 512 nodes per block, i.e. elements per CTA, threads and nodes
-    per thread, and staging depth — by timing the batched step.
+    several occupancies, two element groups ahead, twice the elements per
+    group or two nodes per thread, per-node or (affine meshes, `affine`:
+    default on for precision 32 as in Batch) affine-element geometry, or
+    grouped staging with about 256 / 512 nodes per block, i.e. elements per
+    CTA, threads and nodes per thread, and staging depth — by timing the
+    batched step.
 
     With `instances` (the workload's (dim, N, n_side) list) each shape is
     timed on the workload's own instances of that shape, taken in order up to
@@ -335,6 +360,8 @@ def autotune(precision: int, shapes, nodes_target: int = 4_000_000, steps: int =
     and the chosen variant's launch configuration."""
     torch = _torch()
     from . import ic
+    if affine is None:
+        affine = precision == 32
     best = {}
     if instances is not None:
         for dim, N in shapes:
@@ -360,7 +387,8 @@ def autotune(precision: int, shapes, nodes_target: int = 4_000_000, steps: int =
                     make = (lambda X=X: ic.device_state(list(ic.fourier_state_t(X[0], X[1], X[2], seed=0)), real))
                     dt = 1e-5
                 meshes.append((bm, make, dt))
-            timings = _time_variants(precision, dim, N, meshes, steps, repeat)
+            aff = affine and all(bm.affine for bm, _, _ in meshes)
+            timings = _time_variants(precision, dim, N, meshes, steps, repeat, aff)
             for dm, bm in dms.values():
                 bm.close()
             best[(dim, N)] = min(timings, key=timings.get)
@@ -385,14 +413,18 @@ def autotune(precision: int, shapes, nodes_target: int = 4_000_000, steps: int =
             dt = 1e-5
         real = torch.float64 if precision == 64 else torch.float32
         bm = BatchMesh(dm, precision)
+        aff = affine and bm.affine
         timings = {}
         for var in VARIANTS:
+            if var in AFFINE and not aff:
+                continue
             b = Batch(precision, 1)
             try:
                 b.set_variant(dim, N, var)
             except Exception:
                 b.close()
                 continue
+            b.set_affine(var in AFFINE)
             Q = ic.device_state(list(f), real)
             slot = b.add(bm, Q, torch.zeros_like(Q), dt, 10 ** 9)
             b.run(1)  # build the graph, warm up

@@ -189,7 +189,7 @@ BKernels<T> &b_kernels() {
 }
 template <typename T>
 bool b_var_ok(int dim, int N, int var) {
-  return b_order_ok(dim, N) && var >= 0 && var < NVAR && var != VAR_AFFINE &&
+  return b_order_ok(dim, N) && var >= 0 && var < NVAR &&
          b_kernels<T>().fn[shape_id(dim, N, var)] != nullptr;
 }
 // viscous batches run the grouped two-pass LDG stage (variant 1 shapes)
@@ -198,6 +198,7 @@ constexpr int VAR_VISC = 1;
 // (the autotuner may choose another)
 template <typename T>
 int b_default_var(int dim, int N) {
+  if (dim == 3 && N == 7 && PipeMT<T>::DEFAULT && b_var_ok<T>(dim, N, VAR_MMA)) return VAR_MMA;
   return b_var_ok<T>(dim, N, 0) ? 0 : b_var_ok<T>(dim, N, 2) ? 2 : 1;
 }
 // Shared-memory limit and persistent grid (all SMs at the occupancy that the
@@ -298,8 +299,10 @@ struct cb_batch {
   std::vector<BSlot> slots;
   int64_t steps = 0;  // batch steps launched (the device counter after them)
   int var[2][BMAXN2 + 1] = {};
+  bool var_set[2][BMAXN2 + 1] = {};  // chosen by cb_batch_set_variant (else the default)
   int64_t last_used[NSHAPE] = {};  // batch step at which each shape last had live instances
-  bool affine = true;  // use the affine-element stage where it applies
+  bool affine = true;  // affine-element stages allowed (and the default where they apply)
+  bool concurrent = true;  // shapes as concurrent graph branches (else one chain)
   // one step as a graph; re-built when the set of shapes present changes
   cudaGraphExec_t exec = nullptr;
   std::bitset<NSHAPE> g_shapes;
@@ -389,50 +392,62 @@ cudaError_t build_graph(cb_batch *b, const std::bitset<NSHAPE> &shapes) {
   using SrcArgs = BatchSrc<T, 5, 1>;
   static_assert(sizeof(SrcArgs) == sizeof(BatchSrc<T, 4, 64>) && sizeof(SrcArgs) == sizeof(BatchSrc<T, 4, 64, 4>),
                 "BatchSrc layout");
-  for (int sid = 0; sid < NSHAPE && e == cudaSuccess; ++sid) {
-    if (!shapes.test(sid)) continue;
-    if ((e = b->visc ? b_prepare_visc<T>(sid) : b_prepare<T>(sid)) != cudaSuccess) break;
-    cudaGraphNode_t prev = nullptr;
+  // one kernel node: stage `st` (pass `pass` of a viscous batch) of shape sid
+  auto add = [&](int sid, int st, int pass, cudaGraphNode_t *dep, cudaGraphNode_t *node) {
+    int stage = st;
+    T rka = T(RKA[(st + 1) % 5]);
+    double rkb = RKB[st];
+    PhysT<T> pp = p;
+    SrcArgs src{hdr, sid, st, rkb, nullptr, nullptr, -1};
+    void *gargs[] = {(void *)&hdr, (void *)&stage, (void *)&pp, (void *)&rka, (void *)&rkb};
+    void *pargs[] = {(void *)&src, (void *)&pp, (void *)&rka};
+    cudaKernelNodeParams kp{};
     if (b->visc) {  // per stage: gradient pass, then the stage pass
-      for (int st = 0; st < 5 && e == cudaSuccess; ++st)
-        for (int pass = 0; pass < 2 && e == cudaSuccess; ++pass) {
-          int stage = st;
-          T rka = T(RKA[(st + 1) % 5]);
-          double rkb = RKB[st];
-          PhysT<T> pp = p;
-          void *gargs[] = {(void *)&hdr, (void *)&stage, (void *)&pp, (void *)&rka, (void *)&rkb};
-          cudaKernelNodeParams kp{};
-          kp.func = (void *)K.vfn[pass][sid];
-          kp.gridDim = dim3(K.vgrid[pass][sid]);
-          kp.blockDim = dim3(BT);
-          kp.sharedMemBytes = (unsigned)K.vsmem[pass][sid];
-          kp.kernelParams = gargs;
-          cudaGraphNode_t node;
-          e = cudaGraphAddKernelNode(&node, g, prev ? &prev : nullptr, prev ? 1 : 0, &kp);
-          prev = node;
-        }
-      if (e == cudaSuccess) lasts.push_back(prev);
-      continue;
-    }
-    for (int st = 0; st < 5 && e == cudaSuccess; ++st) {
-      int stage = st;
-      T rka = T(RKA[(st + 1) % 5]);
-      double rkb = RKB[st];
-      PhysT<T> pp = p;
-      SrcArgs src{hdr, sid, st, rkb, nullptr, nullptr, -1};
-      void *gargs[] = {(void *)&hdr, (void *)&stage, (void *)&pp, (void *)&rka, (void *)&rkb};
-      void *pargs[] = {(void *)&src, (void *)&pp, (void *)&rka};
-      cudaKernelNodeParams kp{};
+      kp.func = (void *)K.vfn[pass][sid];
+      kp.gridDim = dim3(K.vgrid[pass][sid]);
+      kp.blockDim = dim3(BT);
+      kp.sharedMemBytes = (unsigned)K.vsmem[pass][sid];
+      kp.kernelParams = gargs;
+    } else {
       kp.func = (void *)K.fn[sid];
       kp.gridDim = dim3(K.grid[sid]);
       kp.blockDim = dim3(K.threads[sid]);
       kp.sharedMemBytes = (unsigned)K.smem[sid];
       kp.kernelParams = K.pipelined[sid] ? pargs : gargs;
-      cudaGraphNode_t node;
-      e = cudaGraphAddKernelNode(&node, g, prev ? &prev : nullptr, prev ? 1 : 0, &kp);
-      prev = node;
     }
-    if (e == cudaSuccess) lasts.push_back(prev);
+    return cudaGraphAddKernelNode(node, g, dep, dep ? 1 : 0, &kp);
+  };
+  std::vector<int> sids;
+  for (int sid = 0; sid < NSHAPE && e == cudaSuccess; ++sid)
+    if (shapes.test(sid)) {
+      sids.push_back(sid);
+      e = b->visc ? b_prepare_visc<T>(sid) : b_prepare<T>(sid);
+    }
+  const int npass = b->visc ? 2 : 1;
+  if (b->concurrent) {
+    // each shape's stages as its own chain, the chains side by side
+    for (int sid : sids) {
+      cudaGraphNode_t prev = nullptr;
+      for (int st = 0; st < 5 && e == cudaSuccess; ++st)
+        for (int pass = 0; pass < npass && e == cudaSuccess; ++pass) {
+          cudaGraphNode_t node;
+          e = add(sid, st, pass, prev ? &prev : nullptr, &node);
+          prev = node;
+        }
+      if (e == cudaSuccess && prev) lasts.push_back(prev);
+    }
+  } else {
+    // one chain: each stage of every shape in turn, so that every kernel has
+    // the whole GPU (persistent grids sized for all SMs do not share them)
+    cudaGraphNode_t prev = nullptr;
+    for (int st = 0; st < 5 && e == cudaSuccess; ++st)
+      for (int sid : sids)
+        for (int pass = 0; pass < npass && e == cudaSuccess; ++pass) {
+          cudaGraphNode_t node;
+          e = add(sid, st, pass, prev ? &prev : nullptr, &node);
+          prev = node;
+        }
+    if (e == cudaSuccess && prev) lasts.push_back(prev);
   }
   if (e == cudaSuccess) {
     BHdr *mh = b->hdr;
@@ -501,12 +516,18 @@ int batch_add(cb_batch *b, const cb_mesh *m, void *Q, void *rhs, double dt, int6
   if (slot < 0) return solver_fail(CB_ERR_NOMEM, "cb_batch_add: all %d slots are in use", b->cap);
   const int Nq = m->N + 1, ns = m->dim == 2 ? 4 : 5;
   const int64_t Np = m->dim == 2 ? (int64_t)Nq * Nq : (int64_t)Nq * Nq * Nq;
-  const int var = b->visc ? VAR_VISC : b->var[m->dim - 2][m->N];
-  int sid = shape_id(m->dim, m->N, var);
+  // the stage variant of the instance: an affine variant runs where the mesh
+  // allows it (else the shape's default per-node variant); a default
+  // pipelined variant is replaced by VAR_AFFINE where the mesh allows it; an
+  // explicitly chosen per-node variant runs as chosen
   const BKernels<T> &K = b_kernels<T>();
-  const bool aff = !b->visc && b->affine && m->affine && b->phys.gravity == 0.0 && K.pipelined[sid] &&
-                   K.fn[shape_id(m->dim, m->N, VAR_AFFINE)];
-  if (aff) sid = shape_id(m->dim, m->N, VAR_AFFINE);
+  const bool eligible = !b->visc && b->affine && m->affine && b->phys.gravity == 0.0;
+  int var = b->visc ? VAR_VISC : b->var[m->dim - 2][m->N];
+  if (var_affine(var) && !eligible) var = b_default_var<T>(m->dim, m->N);
+  else if (!var_affine(var) && eligible && !b->var_set[m->dim - 2][m->N] && K.pipelined[shape_id(m->dim, m->N, var)] &&
+           K.fn[shape_id(m->dim, m->N, VAR_AFFINE)])
+    var = VAR_AFFINE;
+  const int sid = shape_id(m->dim, m->N, var);
   const int epb = K.epb[sid];
   const int64_t ngroups = (m->nelem + epb - 1) / epb;
   const size_t qbytes = sizeof(T) * Np * ns * m->nelem;
@@ -526,7 +547,7 @@ int batch_add(cb_batch *b, const cb_mesh *m, void *Q, void *rhs, double dt, int6
   sl.used = true;
   sl.dim = m->dim;
   sl.N = m->N;
-  sl.var = aff ? VAR_AFFINE : var;
+  sl.var = var;
   sl.sid = sid;
   sl.epb = epb;
   sl.nelem = m->nelem;
@@ -541,7 +562,7 @@ int batch_add(cb_batch *b, const cb_mesh *m, void *Q, void *rhs, double dt, int6
   d.Q[0] = (T *)Q;
   d.Q[1] = (T *)alt;
   d.rhs = (T *)rhs;
-  d.vgeo = (const T *)(aff ? m->aff : m->vgeo);
+  d.vgeo = (const T *)(var_affine(var) ? m->aff : m->vgeo);
   d.sgeo = (const T *)m->sgeo;
   d.D = (const T *)m->D;
   d.nbr = m->nbr;
@@ -783,6 +804,16 @@ int cb_batch_set_variant(cb_batch *b, int dim, int N, int variant) {
     return solver_fail(CB_ERR_UNSUPPORTED, "cb_batch_set_variant: variant %d is not built for dim %d N %d",
                        variant, dim, N);
   b->var[dim - 2][N] = variant;
+  b->var_set[dim - 2][N] = true;
+  return CB_OK;
+}
+
+int cb_batch_set_concurrent(cb_batch *b, int on) {
+  if (!b) return solver_fail(CB_ERR_ARG, "cb_batch_set_concurrent: null handle");
+  if (b->concurrent != (on != 0)) {
+    b->concurrent = on != 0;
+    drop_graph(b);  // re-built at the next run
+  }
   return CB_OK;
 }
 

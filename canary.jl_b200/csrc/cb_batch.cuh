@@ -61,11 +61,15 @@ struct alignas(16) BWork {
 // Stage variants per (dim, N): 0 pipelined (default occupancy), 1 / 2
 // grouped (~256 / ~512 nodes), 3 / 4 pipelined at other occupancies,
 // VAR_DEEP pipelined with copies two groups ahead, VAR_WIDE pipelined with
-// twice the elements per group on 512-thread blocks — the ones a caller may
-// select — and VAR_AFFINE, the pipelined stage with affine-element geometry,
-// which the batch uses in place of a pipelined variant for meshes whose
-// elements are all affine (gravity off).
-constexpr int VAR_AFFINE = 5, VAR_DEEP = 6, VAR_WIDE = 7, NVAR = 8;
+// twice the elements per group on 512-thread blocks, VAR_NPT2 pipelined with
+// two nodes per thread (half the threads), and the affine-element stages
+// (affine-element geometry, copies two groups ahead) VAR_AFFINE and
+// VAR_AFFINE_NPT2 (two nodes per thread).  Affine variants run only on
+// meshes whose elements are all affine (gravity off); by default the batch
+// uses VAR_AFFINE in place of a pipelined variant for such meshes.  VAR_MMA
+// is the tensor-core stage (k_stage_mma, 3-D N = 7).
+constexpr int VAR_AFFINE = 5, VAR_DEEP = 6, VAR_WIDE = 7, VAR_NPT2 = 8, VAR_AFFINE_NPT2 = 9, VAR_MMA = 10, NVAR = 11;
+__host__ __device__ constexpr bool var_affine(int var) { return var == VAR_AFFINE || var == VAR_AFFINE_NPT2; }
 constexpr int NSHAPE = 2 * NVAR * (BMAXN2 + 1);
 __host__ __device__ constexpr int shape_id(int dim, int N, int var) {
   return (dim - 2) * NVAR * (BMAXN2 + 1) + NVAR * N + var;
@@ -631,6 +635,7 @@ struct alignas(16) BRingHdr {
 // writes item it + RING - 1.
 template <typename T, int NS, int EPB, int RING = 3>
 struct BatchSrc {
+  using Real = T;
   static constexpr int WORDS = (int)(sizeof(BDesc<T>) / 8);
   static_assert(sizeof(BDesc<T>) % 8 == 0 && WORDS <= 32, "descriptor words");
   static constexpr int START_WORD = (int)(offsetof(BDesc<T>, start) / 8);
@@ -723,7 +728,7 @@ struct BatchSrc {
   __device__ unsigned *status(int it) const { return at(it).d.status; }
 };
 template <int DIM, int Nq, typename T, int RING = 3, int X = 1>
-using BPipeSrc = BatchSrc<T, Lay<DIM>::NS, CfgX<DIM, Nq, X>::EPB, RING>;
+using BPipeSrc = BatchSrc<T, Lay<DIM>::NS, CfgX<DIM, Nq, X>::EPB, RING>;  // EPB does not depend on Y
 
 inline bool b_order_ok(int dim, int N) { return N >= 1 && N <= (dim == 2 ? BMAXN2 : BMAXN3); }
 
@@ -749,14 +754,14 @@ constexpr size_t b_group_smem() {
   return sizeof(T) * (((Nq * Nq + 1) & ~1) + (size_t)Lay<DIM>::NS * C::SLOTS +
                       (size_t)DIM * Lay<DIM>::NS * C::SLOTS);
 }
-template <int DIM, int Nq, typename T, int MINB, bool AFF = false, bool DEEP = false, int X = 1>
+template <int DIM, int Nq, typename T, int MINB, bool AFF = false, bool DEEP = false, int X = 1, int Y = 1>
 void b_fill_pipe(BKernels<T> &k, int var) {
   using Src = BPipeSrc<DIM, Nq, T, DEEP ? 4 : 3, X>;
   const int id = shape_id(DIM, Nq - 1, var);
-  k.fn[id] = (const void *)k_stage_pipe2<DIM, Nq, T, Src, MINB, AFF, DEEP, X>;
-  k.epb[id] = CfgX<DIM, Nq, X>::EPB;
-  k.threads[id] = CfgX<DIM, Nq, X>::THREADS;
-  k.smem[id] = Pipe2<DIM, Nq, T, AFF, DEEP, X>::smem() + Src::RING_BYTES;
+  k.fn[id] = (const void *)k_stage_pipe2<DIM, Nq, T, Src, MINB, AFF, DEEP, X, Y>;
+  k.epb[id] = CfgX<DIM, Nq, X, Y>::EPB;
+  k.threads[id] = CfgX<DIM, Nq, X, Y>::THREADS;
+  k.smem[id] = Pipe2<DIM, Nq, T, AFF, DEEP, X, Y>::smem() + Src::RING_BYTES;
   k.pipelined[id] = true;
   k.ahead[id] = DEEP ? 2 : 1;
 }
@@ -784,6 +789,26 @@ void b_fill(BKernels<T> &k) {
     using PD = Pipe2<DIM, Nq, T, true, true>;
     if constexpr (PD::OK && PD::fits(M0)) b_fill_pipe<DIM, Nq, T, M0, true, true>(k, VAR_AFFINE);
     else if constexpr (Pipe2<DIM, Nq, T, true>::OK) b_fill_pipe<DIM, Nq, T, M0, true>(k, VAR_AFFINE);
+    // the tensor-core stage (3-D N = 7, one element per group)
+    if constexpr (DIM == 3 && Nq == 8) {
+      using PM = PipeMT<T>;
+      using Src = BatchSrc<T, 5, 1, 3>;
+      const int id = shape_id(DIM, N, VAR_MMA);
+      k.fn[id] = (const void *)k_stage_mma<Src, PM::MINB>;
+      k.epb[id] = 1;
+      k.threads[id] = PM::THREADS;
+      k.smem[id] = PM::smem() + Src::RING_BYTES;
+      k.pipelined[id] = true;
+      k.ahead[id] = 1;
+    }
+    // two nodes per thread on half the threads (blocks of 128 or more), per-node
+    // and affine geometry, as many blocks per SM as shared memory holds
+    if constexpr (Cfg<DIM, Nq>::THREADS >= 256) {
+      using PY = Pipe2<DIM, Nq, T, false, false, 1, 2>;
+      if constexpr (PY::OK && PY::fits(PY::MINB)) b_fill_pipe<DIM, Nq, T, PY::MINB, false, false, 1, 2>(k, VAR_NPT2);
+      using PA = Pipe2<DIM, Nq, T, true, true, 1, 2>;
+      if constexpr (PA::OK && PA::fits(PA::MINB)) b_fill_pipe<DIM, Nq, T, PA::MINB, true, true, 1, 2>(k, VAR_AFFINE_NPT2);
+    }
   }
   {
     const int id = shape_id(DIM, N, 1);

@@ -77,15 +77,17 @@ struct Cfg {
   static constexpr int FPT = cdiv(FSLOTS, THREADS);
 };
 
-// The same with X times the elements per group and X times the threads (the
-// same nodes per thread): larger groups share each block barrier among more
-// nodes.  X = 1 is Cfg.
-template <int DIM, int Nq, int X>
+// The same with X times the elements per group on X / Y times the threads:
+// X > 1 shares each block barrier among more nodes, Y > 1 gives each thread
+// Y times the nodes (more independent work per thread, the per-group
+// bookkeeping spread over more nodes).  X = Y = 1 is Cfg.
+template <int DIM, int Nq, int X, int Y = 1>
 struct CfgX : Cfg<DIM, Nq> {
   using B = Cfg<DIM, Nq>;
   static constexpr int EPB = B::EPB * X;
   static constexpr int SLOTS = EPB * B::Np;
-  static constexpr int THREADS = B::THREADS * X;
+  static constexpr int THREADS =
+      Y == 1 ? B::THREADS * X : (cdiv(B::THREADS * X / Y, 32) * 32 < 64 ? 64 : cdiv(B::THREADS * X / Y, 32) * 32);
   static constexpr int NPT = cdiv(SLOTS, THREADS);
   static constexpr int FSLOTS = EPB * B::NFACE * B::Nfp;
   static constexpr int FPT = cdiv(FSLOTS, THREADS);

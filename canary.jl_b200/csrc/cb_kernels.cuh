@@ -797,10 +797,10 @@ struct Launch {
     return cudaGetLastError();
   }
   // Whether the tensor-core (DMMA) stage is built for this shape.
-  static constexpr bool MMA_OK = DIM == 3 && Nq == 8 && sizeof(T) == 8;
+  static constexpr bool MMA_OK = DIM == 3 && Nq == 8;
   // Whether kernel 0 (the shape's default) is the tensor-core stage: the
   // faster of the two on B200 at the benchmark size.
-  static constexpr bool MMA_DEFAULT = MMA_OK && PipeM::DEFAULT;
+  static constexpr bool MMA_DEFAULT = MMA_OK && PipeMT<T>::DEFAULT;
   // Resident blocks per SM of a kernel at `smem` bytes, from the occupancy
   // calculator, cached per device in `cache`.
   template <typename K>
@@ -842,15 +842,16 @@ struct Launch {
     if (groups == 0) return cudaSuccess;
     if constexpr (MMA_OK) {
       if ((kernel == 2 || (kernel == 0 && MMA_DEFAULT)) && aligned2) {
-        using S = MeshSrc<T, NS, C::EPB>;  // MeshSrc<double, 5, 1> here
+        using S = MeshSrc<T, NS, C::EPB>;  // MeshSrc<T, 5, 1> here
+        using PM = PipeMT<T>;
         static int per_sm[MAX_DEVICES] = {0};
         int bps = 0;
-        cudaError_t err = blocks_per_sm(k_stage_mma<S, PipeM::MINB>, PipeM::THREADS, PipeM::smem(), per_sm, &bps);
+        cudaError_t err = blocks_per_sm(k_stage_mma<S, PM::MINB>, PM::THREADS, PM::smem(), per_sm, &bps);
         if (err != cudaSuccess) return err;
         int64_t g = (int64_t)num_sms() * bps;
         if (g > groups) g = groups;
         const S src{Qin, Qout, rhs, vgeo, sgeo, nbr, D, nelem, qref, rkbdt, status, probe, ebeg};
-        k_stage_mma<S, PipeM::MINB><<<(int)g, PipeM::THREADS, PipeM::smem(), st>>>(src, p, rka);
+        k_stage_mma<S, PM::MINB><<<(int)g, PM::THREADS, PM::smem(), st>>>(src, p, rka);
         return cudaGetLastError();
       }
     }

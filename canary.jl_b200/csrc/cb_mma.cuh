@@ -1,6 +1,7 @@
 // Fused LSRK stage with the D contraction on the FP64 tensor cores (sm_100a).
 //
-// 3-D hexahedra at N = 7 (Nq = 8, 512 nodes per element), FP64.  The same
+// 3-D hexahedra at N = 7 (Nq = 8, 512 nodes per element), FP64 and FP32
+// storage (the contraction in FP64 either way).  The same
 // stage as k_stage_pipe2 (volume + Rusanov face + LSRK update, state read
 // from one buffer and written to the other), with a different division of
 // the work inside an element:
@@ -49,14 +50,19 @@ __device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes) {
 }
 
 // Shared-memory plan of the tensor-core stage (per block, one element per
-// group).
-struct PipeM {
+// group) for state, geometry and carry stored in T.  The flux planes are
+// FP64 in either case: the FP32 form (T = float) computes its fluxes in
+// FP32, contracts them with D on the FP64 tensor pipe (products of FP32
+// values are exact in FP64, the sums are rounded once) and rounds the
+// result to FP32.
+template <typename T>
+struct PipeMT {
   static constexpr int DIM = 3, Nq = 8, Np = 512, Nfp = 64, NF = 6, NS = 5, NVG = 14, NSG = 5;
   static constexpr int THREADS = 256, WARPS = 8;
   static constexpr int FSLOTS = NF * Nfp, FPT = (FSLOTS + THREADS - 1) / THREADS;
-  static constexpr size_t QB = sizeof(double) * Np * NS;             // state slab (bulk copy)
-  static constexpr size_t GB = sizeof(double) * Np * (DIM * DIM + 2);  // metric, MJ, MJI (L2 prefetch)
-  static constexpr size_t SB = sizeof(double) * NSG * Nfp * NF;      // face geometry (L2 prefetch)
+  static constexpr size_t QB = sizeof(T) * Np * NS;             // state slab (bulk copy)
+  static constexpr size_t GB = sizeof(T) * Np * (DIM * DIM + 2);  // metric, MJ, MJI (L2 prefetch)
+  static constexpr size_t SB = sizeof(T) * NSG * Nfp * NF;      // face geometry (L2 prefetch)
   // F and G planes of one warp: [NS][2][64] (row j, swizzled column i)
   static constexpr int FGW = NS * 2 * 64;
   // H (then the zeta products in place): [NS][8 planes][68], planes padded so
@@ -66,7 +72,7 @@ struct PipeM {
   static constexpr size_t OFF_FG = OFF_S + QB;
   static constexpr size_t OFF_HZ = OFF_FG + sizeof(double) * WARPS * FGW;
   static constexpr size_t OFF_FF = OFF_HZ + sizeof(double) * NS * HS;
-  static constexpr size_t FFB = sizeof(double) * NF * NS * Nfp;
+  static constexpr size_t FFB = sizeof(T) * NF * NS * Nfp;
   static constexpr size_t smem() { return OFF_FF + FFB; }  // item sources append their ring here
   // PFD = -1: each group's metric, carry and face geometry are prefetched
   // into L2 at the top of its own iteration.  Measured on B200 (16^3-hex
@@ -76,9 +82,22 @@ struct PipeM {
   // reads 1.00x and is the fastest (127.6 us against 135 us without a
   // prefetch and 162 us for the CUDA-core stage).
   static constexpr int MINB = 2, PFD = -1;
-  // whether this stage is the default of its shape (the faster on B200: at
-  // 32^3 hexes 0.997 ms per stage against 1.18 ms for the CUDA-core stage)
+  // whether this stage is the default of its shape (the faster on B200 at
+  // 32^3 hexes: FP64 0.974 ms per stage against 1.17 ms for the CUDA-core
+  // stage, FP32 0.719 against 0.744 ms)
   static constexpr bool DEFAULT = true;
+};
+using PipeM = PipeMT<double>;
+
+template <typename T>
+struct Vec2;
+template <>
+struct Vec2<double> {
+  using type = double2;
+};
+template <>
+struct Vec2<float> {
+  using type = float2;
 };
 
 // Position of (i, j) in an 8 x 8 plane (a warp's F or G plane, a plane of
@@ -93,19 +112,22 @@ __device__ __forceinline__ int fg_pos(int i, int j) { return j * 8 + (i ^ (((j >
 // geometry is issued (0: none, the loads go to HBM directly; -1: for the
 // group itself, at the top of its iteration).
 template <typename Src, int MINB = PipeM::MINB, int PFD = PipeM::PFD>
-__global__ void __launch_bounds__(PipeM::THREADS, MINB) k_stage_mma(Src src, PhysT<double> p, double rka) {
-  using PM = PipeM;
-  using T = double;
+__global__ void __launch_bounds__(PipeM::THREADS, MINB)
+    k_stage_mma(Src src, PhysT<typename Src::Real> p, typename Src::Real rka) {
+  using T = typename Src::Real;  // storage (and, for float, flux and update arithmetic)
+  using A = double;              // flux planes and tensor-core products
+  using V2 = typename Vec2<T>::type;
+  using PM = PipeMT<T>;
   constexpr int DIM = 3, Nq = 8, Np = 512, Nfp = 64, NF = 6, NS = 5, NVG = 14, NSG = 5, IR = 3;
   constexpr int MJF = DIM * DIM, MJIF = DIM * DIM + 1, GC = DIM * DIM + 2 + DIM - 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   uint64_t *barS = reinterpret_cast<uint64_t *>(smem_raw);
   T *S = reinterpret_cast<T *>(smem_raw + PM::OFF_S);
-  T *FGall = reinterpret_cast<T *>(smem_raw + PM::OFF_FG);
-  T *HZ = reinterpret_cast<T *>(smem_raw + PM::OFF_HZ);
+  A *FGall = reinterpret_cast<A *>(smem_raw + PM::OFF_FG);
+  A *HZ = reinterpret_cast<A *>(smem_raw + PM::OFF_HZ);
   T *FF = reinterpret_cast<T *>(smem_raw + PM::OFF_FF);
   const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
-  T *FG = FGall + w * PM::FGW;
+  A *FG = FGall + w * PM::FGW;
   const int n0 = 2 * t + 8 * g + 64 * w;  // the lane's nodes n0, n0 + 1
 
   auto issue_S = [&](int it) {  // thread 0 only
@@ -146,7 +168,7 @@ __global__ void __launch_bounds__(PipeM::THREADS, MINB) k_stage_mma(Src src, Phy
   load_nbr(0, nbn);
 
   const T *curD = nullptr;
-  T Dg0 = T(0), Dg1 = T(0);  // D[t, g] and D[t + 4, g] (column-major D[m + Nq i])
+  A Dg0 = A(0), Dg1 = A(0);  // D[t, g] and D[t + 4, g] (column-major D[m + Nq i])
   bool timed_out = false;
   for (int it = 0; src.valid(it); ++it) {
     const int64_t e0 = src.e0(it);
@@ -162,8 +184,8 @@ __global__ void __launch_bounds__(PipeM::THREADS, MINB) k_stage_mma(Src src, Phy
     for (int s = 0; s < NS; ++s) qr[s] = src.qref(it, s);
     if (src.D(it) != curD) {
       curD = src.D(it);
-      Dg0 = curD[t + Nq * g];
-      Dg1 = curD[t + 4 + Nq * g];
+      Dg0 = A(curD[t + Nq * g]);
+      Dg1 = A(curD[t + 4 + Nq * g]);
     }
 
     // ---- loads that do not need the staged state: neighbour traces and
@@ -232,9 +254,9 @@ __global__ void __launch_bounds__(PipeM::THREADS, MINB) k_stage_mma(Src src, Phy
     // ---- volume fluxes of the lane's two nodes, one node at a time: F, G
     // into the warp's planes, H into the shared zeta buffer (the metric is
     // loaded here, after the face phase, whose registers it would crowd)
-    double2 met[DIM * DIM + 1];
+    V2 met[DIM * DIM + 1];
 #pragma unroll
-    for (int f = 0; f <= MJF; ++f) met[f] = *reinterpret_cast<const double2 *>(vg + n0 + Np * f);
+    for (int f = 0; f <= MJF; ++f) met[f] = *reinterpret_cast<const V2 *>(vg + n0 + Np * f);
     T qd[2][NS], buoy[2];
 #pragma unroll
     for (int c = 0; c < 2; ++c) {
@@ -263,18 +285,18 @@ __global__ void __launch_bounds__(PipeM::THREADS, MINB) k_stage_mma(Src src, Phy
         for (int s = 0; s < NS; ++s) {
           T a = mt[r][0] * f[s][0] + mt[r][1] * f[s][1];
           a = a + mt[r][2] * f[s][2];
-          T *dst = r < 2 ? FG + (s * 2 + r) * 64 : HZ + s * PM::HS + w * PM::HP;
-          dst[pf] = MJ * a;
+          A *dst = r < 2 ? FG + (s * 2 + r) * 64 : HZ + s * PM::HS + w * PM::HP;
+          dst[pf] = A(MJ * a);
         }
       buoy[c] = MJ * q[IR] * p.grav;
     }
     __syncwarp();
     // ---- xi and eta products of this warp's plane (warp-private planes)
-    T acc[NS][2];
+    A acc[NS][2];
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
-      const T *Fp = FG + (s * 2 + 0) * 64, *Gp = FG + (s * 2 + 1) * 64;
-      T c0 = T(0), c1 = T(0);
+      const A *Fp = FG + (s * 2 + 0) * 64, *Gp = FG + (s * 2 + 1) * 64;
+      A c0 = A(0), c1 = A(0);
       // xi: C[j][i] += Σ_m F[m, j]·D[m, i]   (A = F_kᵀ, B = D)
       dmma(c0, c1, Fp[fg_pos(t, g)], Dg0, c0, c1);
       dmma(c0, c1, Fp[fg_pos(t + 4, g)], Dg1, c0, c1);
@@ -302,20 +324,20 @@ __global__ void __launch_bounds__(PipeM::THREADS, MINB) k_stage_mma(Src src, Phy
     // writes them over the H values it has just read (the same positions)
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
-      T *Hs = HZ + s * PM::HS;
+      A *Hs = HZ + s * PM::HS;
       const int pz = fg_pos(g, w);
-      const T a0 = Hs[t * PM::HP + pz], a1 = Hs[(t + 4) * PM::HP + pz];
-      T z0 = T(0), z1 = T(0);
+      const A a0 = Hs[t * PM::HP + pz], a1 = Hs[(t + 4) * PM::HP + pz];
+      A z0 = A(0), z1 = A(0);
       dmma(z0, z1, a0, Dg0, z0, z1);
       dmma(z0, z1, a1, Dg1, z0, z1);
       Hs[(2 * t) * PM::HP + pz] = z0;
       Hs[(2 * t + 1) * PM::HP + pz] = z1;
     }
     // residual carry and 1/MJ of the lane's nodes
-    double2 cr[NS];
+    V2 cr[NS];
 #pragma unroll
-    for (int s = 0; s < NS; ++s) cr[s] = *reinterpret_cast<const double2 *>(rhs + n0 + Np * s);
-    const double2 mji = *reinterpret_cast<const double2 *>(vg + n0 + Np * MJIF);
+    for (int s = 0; s < NS; ++s) cr[s] = *reinterpret_cast<const V2 *>(rhs + n0 + Np * s);
+    const V2 mji = *reinterpret_cast<const V2 *>(vg + n0 + Np * MJIF);
     __syncthreads();  // zeta products complete
 
     // ---- carry - source + products - face terms, update
@@ -333,8 +355,8 @@ __global__ void __launch_bounds__(PipeM::THREADS, MINB) k_stage_mma(Src src, Phy
 #pragma unroll
       for (int c = 0; c < 2; ++c) {
         if (s == DIM - 1) R[c] -= buoy[c];
-        R[c] += acc[s][c];
-        R[c] += c ? z.y : z.x;
+        R[c] += T(acc[s][c]);
+        R[c] += T(c ? z.y : z.x);
         const int i = 2 * t + c;
         if (i == 0) R[c] -= FF[(0 * NS + s) * Nfp + j + Nq * k];
         if (i == Nq - 1) R[c] -= FF[(1 * NS + s) * Nfp + j + Nq * k];
@@ -345,8 +367,8 @@ __global__ void __launch_bounds__(PipeM::THREADS, MINB) k_stage_mma(Src src, Phy
       }
       const T q0 = qd[0][s] + rkbdt * R[0] * mji.x, q1 = qd[1][s] + rkbdt * R[1] * mji.y;
       bad |= !isfinite(q0) || !isfinite(q1);
-      *reinterpret_cast<double2 *>(Qout + n0 + Np * s) = make_double2(q0, q1);
-      *reinterpret_cast<double2 *>(rhs + n0 + Np * s) = make_double2(R[0] * rka, R[1] * rka);
+      *reinterpret_cast<V2 *>(Qout + n0 + Np * s) = V2{q0, q1};
+      *reinterpret_cast<V2 *>(rhs + n0 + Np * s) = V2{R[0] * rka, R[1] * rka};
     }
     if (bad) atomicOr(src.status(it), ST_NONFINITE);
     __syncthreads();  // FF, the zeta buffer and the item ring are free for reuse

@@ -50,11 +50,11 @@ namespace cb {
 // about twice the bytes in flight, for small groups whose copy latency a
 // single group of work does not cover.
 //
-// X: X times the elements per group of Cfg, on X times the threads (the same
-// nodes per thread), so that each block barrier is shared by more nodes.
-template <int DIM, int Nq, typename T, bool AFF = false, bool DEEP = false, int X = 1>
+// X, Y: X times the elements per group of Cfg on X / Y times the threads
+// (CfgX): each block barrier shared by more nodes, or Y nodes per thread.
+template <int DIM, int Nq, typename T, bool AFF = false, bool DEEP = false, int X = 1, int Y = 1>
 struct Pipe2 {
-  using C = CfgX<DIM, Nq, X>;
+  using C = CfgX<DIM, Nq, X, Y>;
   using P1 = Pipe<DIM, Nq, T, X>;
   static constexpr int NS = Lay<DIM>::NS, NSG = Lay<DIM>::NSG, NVG = Lay<DIM>::NVG;
   static constexpr int NG = P1::NG, RS = P1::RS, NR = P1::NR, MV = P1::MV;
@@ -75,11 +75,12 @@ struct Pipe2 {
   static constexpr size_t QBS = pad16(C::EPB * QB + SLK);            // staged state / carry per slab
   static constexpr size_t SGS = AFF ? 0 : pad16(C::EPB * SB + SLK);  // staged sgeo per slab
   static constexpr bool BULK = AFF || pad16(GB) + 16 <= VB;
-  static constexpr int NSB = DEEP ? 2 : 1, NTB = DEEP ? 3 : 2;  // S and T slabs
   static constexpr int LOOK = DEEP ? 2 : 1;  // groups ahead whose copies are issued
-  static constexpr size_t OFF_D = DEEP ? 48 : 32;  // NSB + NTB mbarriers before
-  // D rows, then (AFF) the LGL weights
-  static constexpr size_t OFF_S = OFF_D + pad16(sizeof(T) * Nq * RS) + (AFF ? pad16(sizeof(T) * Nq) : 0);
+  static constexpr int NSB = DEEP ? 2 : 1, NTB = LOOK + 1;  // S and T slabs
+  static constexpr size_t OFF_D = pad16(8 * (NSB + NTB));  // the mbarriers before
+  // D rows (DTS elements), then (AFF) the LGL weights
+  static constexpr size_t DTS = pad16(sizeof(T) * Nq * RS) / sizeof(T);
+  static constexpr size_t OFF_S = OFF_D + sizeof(T) * DTS + (AFF ? pad16(sizeof(T) * Nq) : 0);
   static constexpr size_t SBYTES = QBS + C::EPB * GBP;
   static constexpr size_t OFF_T = OFF_S + NSB * pad16(SBYTES);
   static constexpr size_t TBYTES = QBS + SGS;
@@ -91,19 +92,28 @@ struct Pipe2 {
   static constexpr size_t smem() { return OFF_FF + pad16(FFB); }  // sources append their ring here
   static constexpr size_t RING_MAX = 640;
   static constexpr bool OK = BULK && smem() + RING_MAX <= SMEM_LIMIT;
-  // blocks of up to 256 threads are sized for two (FP64) or four (FP32) per SM
-  // (larger groups of X > 1: 512-thread FP32 blocks two per SM)
-  static constexpr int MINB =
-      C::THREADS <= 256 ? (sizeof(T) == 4 ? 4 : 2) : (X > 1 && C::THREADS <= 512 && sizeof(T) == 4 ? 2 : 1);
   // whether `blocks` blocks fit in one SM's shared memory (228 KB, 1 KB of
   // it reserved per block)
   static constexpr bool fits(int blocks) { return blocks * (smem() + RING_MAX + 1024) <= 228 * 1024; }
+  // Y > 1: as many blocks per SM as shared memory holds, up to 2048 threads
+  // and at least 72 registers per thread
+  static constexpr int minb_fit() {
+    int b = 1;
+    while (b < 8 && fits(b + 1) && (b + 1) * C::THREADS <= 2048 && (b + 1) * C::THREADS * 72 <= 65536) ++b;
+    return b;
+  }
+  // blocks of up to 256 threads are sized for two (FP64) or four (FP32) per SM
+  // (larger groups of X > 1: 512-thread FP32 blocks two per SM)
+  static constexpr int MINB =
+      Y > 1 ? minb_fit()
+            : C::THREADS <= 256 ? (sizeof(T) == 4 ? 4 : 2) : (X > 1 && C::THREADS <= 512 && sizeof(T) == 4 ? 2 : 1);
 };
 
 // One mesh: groups of EPB consecutive elements, pointers and constants are
 // kernel parameters.
 template <typename T, int NS, int EPB>
 struct MeshSrc {
+  using Real = T;
   static constexpr size_t RING_BYTES = 0;
   static constexpr int PUBLISHER = 0;
   static constexpr int AHEAD = 1 << 20;  // groups ahead known at the top of an iteration
@@ -152,13 +162,14 @@ struct MeshSrc {
 
 // MINB: resident blocks per SM that the register allocation is sized for;
 // AFF: affine-element geometry (see Pipe2; gravity must be zero); DEEP:
-// copies two groups ahead (see Pipe2); X: X times the elements per group.
+// copies two groups ahead (see Pipe2); X, Y: X times the elements per group
+// on X / Y times the threads.
 template <int DIM, int Nq, typename T, typename Src, int MINB = Pipe2<DIM, Nq, T>::MINB, bool AFF = false,
-          bool DEEP = false, int X = 1>
-__global__ void __launch_bounds__(CfgX<DIM, Nq, X>::THREADS, MINB)
+          bool DEEP = false, int X = 1, int Y = 1>
+__global__ void __launch_bounds__(CfgX<DIM, Nq, X, Y>::THREADS, MINB)
 k_stage_pipe2(Src src, PhysT<T> p, T rka) {
-  using C = CfgX<DIM, Nq, X>;
-  using PP = Pipe2<DIM, Nq, T, AFF, DEEP, X>;
+  using C = CfgX<DIM, Nq, X, Y>;
+  using PP = Pipe2<DIM, Nq, T, AFF, DEEP, X, Y>;
   static_assert(Src::AHEAD >= PP::LOOK, "the source must publish the groups whose copies are issued");
   constexpr int NS = Lay<DIM>::NS, NVG = Lay<DIM>::NVG, NSG = Lay<DIM>::NSG, IR = Lay<DIM>::IR;
   constexpr int Np = C::Np, Nfp = C::Nfp, NF = C::NFACE, EPB = C::EPB, SP = C::SLOTS;
@@ -270,7 +281,7 @@ k_stage_pipe2(Src src, PhysT<T> p, T rka) {
   load_nbr(0, nbn);
   // AFF: the LGL weights head every mesh's record array (the same for every
   // mesh of this order)
-  const T *WS = DT + Nq * RS;
+  const T *WS = DT + PP::DTS;
   if constexpr (AFF) {
     if (tid < Nq && src.valid(0)) const_cast<T *>(WS)[tid] = src.vgeo(0)[tid];
     __syncthreads();

@@ -187,8 +187,9 @@ int cb_solver_status_async(cb_solver *s, unsigned *out_host);
 /* Stage kernel of the inviscid form: 0 = the default for the shape, 1 = the
  * CUDA-core stages (pipelined bulk-copy staging where the plan fits), 2 = the
  * tensor-core stage (D contraction on the FP64 tensor pipe as 8x8x4 DMMA
- * tiles; built for 3-D N=7 FP64, CB_ERR_UNSUPPORTED elsewhere).  The default
- * is whichever of the two is faster on B200 for the shape.  Both agree with
+ * tiles, for FP32 solvers on the FP32 fluxes converted to FP64, the sum
+ * rounded once; built for 3-D N=7, CB_ERR_UNSUPPORTED elsewhere).  The
+ * default is whichever of the two is faster on B200 for the shape.  Both agree with
  * the oracle to round-off; changing it re-captures the step graph at the
  * next run.
  * cb_solver_get_kernel reports the kernel the solver runs (1 or 2). */
@@ -345,26 +346,42 @@ int cb_batch_create(cb_batch **out, int precision, int max_instances,
  * compiled for the other occupancies (2, 3 or 4 blocks per SM), 6 = pipelined
  * staging with copies two element groups ahead instead of one, 7 = pipelined
  * staging with twice the elements per group on twice the threads (shapes
- * whose default block has at most 256 threads).  Variants
- * that are not built for (dim, N) give CB_ERR_UNSUPPORTED.  Chosen by an
- * autotuner; the pipelined variants agree bit for bit among themselves, as do
- * the grouped ones, and the two families to round-off. */
+ * whose default block has at most 256 threads), 8 = pipelined staging with
+ * two nodes per thread on half the threads; 5 and 9 = the affine-element
+ * stage (see cb_batch_set_affine; copies two groups ahead) with one and two
+ * nodes per thread; 10 = the tensor-core stage (3-D N=7, as
+ * cb_solver_set_kernel 2; the default there for precision 64).  An affine
+ * variant (5, 9) runs on meshes that allow it and falls back to the shape's
+ * default per-node variant elsewhere.  A variant
+ * chosen here runs as chosen; without a choice the batch uses variant 5 in
+ * place of its default pipelined variant where the affine stage applies.
+ * Variants that are not built for (dim, N) give CB_ERR_UNSUPPORTED.  Chosen
+ * by an autotuner; the per-node pipelined variants agree bit for bit among
+ * themselves, as do the grouped ones and the affine ones, and the families
+ * to round-off. */
 int cb_batch_set_variant(cb_batch *b, int dim, int N, int variant);
 int cb_batch_get_variant(const cb_batch *b, int dim, int N, int *variant);
 /* Launch configuration of a stage variant of (dim, N) in this batch's
- * precision (5: the affine-element stage): info[0] elements per CTA,
+ * precision: info[0] elements per CTA,
  * info[1] threads per CTA, info[2] nodes per thread, info[3] element groups
  * staged ahead of the work (0: grouped staging, no copies in flight),
  * info[4] resident CTAs per SM, info[5] dynamic shared memory per CTA. */
 int cb_batch_variant_info(const cb_batch *b, int dim, int N, int variant, int64_t *info);
-/* Instances admitted from now on whose mesh is affine (cb_mesh_affine), with
- * gravity 0 and a pipelined variant selected, use the affine-element stage
- * when `on`; it reads no vgeo / sgeo and uses each element's first-node
- * metric for all its nodes, which agrees with the per-node geometry to
- * round-off per stage.  Default: on for precision 32, off for precision 64
- * (over hundreds of FP64 steps that round-off reaches ~1e-11 relative,
- * above the 1e-12 oracle bar). */
+/* Whether instances admitted from now on whose mesh is affine
+ * (cb_mesh_affine), with gravity 0, may use the affine-element stage: an
+ * affine variant chosen by cb_batch_set_variant, or variant 5 in place of a
+ * default pipelined variant.  The stage reads no vgeo / sgeo and uses each
+ * element's first-node metric for all its nodes, which agrees with the
+ * per-node geometry to round-off per stage.  Default: on for precision 32,
+ * off for precision 64 (over hundreds of FP64 steps that round-off reaches
+ * ~1e-11 relative, above the 1e-12 oracle bar). */
 int cb_batch_set_affine(cb_batch *b, int on);
+/* How the step graph orders the shapes present: 1 (default) = one chain per
+ * shape, the chains as concurrent graph branches (kernels of different
+ * shapes share the SMs); 0 = one chain, each RK stage of every shape in
+ * turn, so that each persistent stage kernel has the whole GPU.  Results do
+ * not depend on it. */
+int cb_batch_set_concurrent(cb_batch *b, int on);
 /* Admit an instance: the caller's state Q and zeroed residual carry rhs
  * (layouts as above, precision of the batch) advance by nsteps steps of dt
  * during the following cb_batch_run calls.  qref (nstate doubles, or NULL for
@@ -380,8 +397,8 @@ int cb_batch_add(cb_batch *b, const cb_mesh *m, void *Q, void *rhs, double dt,
 int cb_batch_run(cb_batch *b, int64_t nsteps);
 /* Steps taken and to take by a slot (host bookkeeping, no synchronisation). */
 int cb_batch_info(const cb_batch *b, int slot, int64_t *done, int64_t *target);
-/* Stage variant an admitted slot runs with: the variant selected for its
- * (dim, N) when it was admitted, or 5 for the affine-element stage. */
+/* Stage variant an admitted slot runs with (the variant in effect for its
+ * (dim, N) when it was admitted, after the affine rules above). */
 int cb_batch_slot_variant(const cb_batch *b, int slot, int *variant);
 /* Retire a slot: the instance's current state is placed in its Q (stream-
  * ordered), the twin buffer returns to the pool and the slot is free. */

@@ -112,5 +112,6 @@ def test_partition_and_setup_argument_validation_without_device():
     assert L.cb_brickmesh(3, 3, bad, xs, per, None, dummy, dummy, dummy, dummy, None) == _lib.CB_ERR_ARG
     assert L.cb_mesh_affine(None, None) == _lib.CB_ERR_ARG
     assert L.cb_batch_set_affine(None, 1) == _lib.CB_ERR_ARG
+    assert L.cb_batch_set_concurrent(None, 1) == _lib.CB_ERR_ARG
     assert L.cb_batch_slot_variant(None, 0, None) == _lib.CB_ERR_ARG
 

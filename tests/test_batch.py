@@ -45,11 +45,16 @@ def oracle_results(cases):
     return [oracle_run(m, Q, dt, k) for (m, Q, dt, k) in cases]
 
 
-def _run_batch(cases, precision, idx=None, chunks=(2, 3, 100), variants=None):
+def _run_batch(cases, precision, idx=None, chunks=(2, 3, 100), variants=None, affine=None, used=False,
+               concurrent=None):
     """Admit cases[idx] into one batch, run in the given chunks, return the
-    final FP64 host states."""
+    final FP64 host states (and, with `used`, the variant each slot ran)."""
     idx = range(len(cases)) if idx is None else idx
     b = B.Batch(precision, max_instances=64)
+    if affine is not None:
+        b.set_affine(affine)
+    if concurrent is not None:
+        b.set_concurrent(concurrent)
     for (dim, N, v) in (variants or []):
         b.set_variant(dim, N, v)
     meshes, slots = [], []
@@ -58,12 +63,13 @@ def _run_batch(cases, precision, idx=None, chunks=(2, 3, 100), variants=None):
         bm = B.BatchMesh(dg.DeviceMesh.upload(m), precision)
         meshes.append(bm)
         slots.append(b.add_state(bm, Q, dt, k))
+    ran = [b.slot_variant(s) for s in slots]
     for c in chunks:
         b.run(c)
     assert not b.status().any()
     out = [b.result(s) for s in slots]
     b.close()
-    return out
+    return (out, ran) if used else out
 
 
 def test_batch_fp64_matches_oracle(cases, oracle_results):
@@ -91,9 +97,14 @@ def test_batch_result_same_alone_and_in_mix(cases, precision):
 @pytest.mark.parametrize("precision", [64, 32])
 def test_batch_variants_agree(cases, precision):
     """Grouped variants (1, 2) are bit-identical to each other, and so are the
-    pipelined ones (0, 3, 4, 6, 7: the same code at other occupancies, staging
-    depth or group size); the two families sum the contraction differently
-    (padded rows) and agree to round-off."""
+    per-node pipelined ones (0, 3, 4, 6, 7, 8: the same code at other
+    occupancies, staging depth, group size or nodes per thread) and the
+    affine ones (5, 9) on affine meshes; the families sum the contraction
+    (padded rows) or form the geometry differently and agree to round-off:
+    1e-13 (FP64) / 1e-5 (FP32) relative between the per-node families,
+    1e-11 / 1e-5 for the affine stage.  A chosen variant runs as chosen: a
+    per-node one is not replaced by the affine stage, an affine one falls back
+    to the default per-node variant on a warped mesh."""
     orders = [(m.dim, m.N) for (m, Q, dt, k) in cases]
     probe = B.Batch(precision, 1)
     built = {}
@@ -105,18 +116,42 @@ def test_batch_variants_agree(cases, precision):
             except CanaryError:
                 built[(d, N, v)] = False
     probe.close()
-    runs = {}
+    runs, used = {}, {}
     for v in B.VARIANTS:
-        runs[v] = _run_batch(cases, precision, variants=[(d, N, v) for d, N in orders if built[(d, N, v)]])
+        runs[v], used[v] = _run_batch(cases, precision, variants=[(d, N, v) for d, N in orders if built[(d, N, v)]],
+                                      affine=True, used=True)
     tol = 1e-13 if precision == 64 else 1e-5
+    tol_aff = 1e-11 if precision == 64 else 1e-5
     for i, (m, Q, dt, k) in enumerate(cases):
+        affine = m.dim == 2  # uniform vortex meshes; the 3-D Fourier cubes are warped
+        for v in B.VARIANTS:
+            if built[(m.dim, m.N, v)] and v not in B.AFFINE:
+                assert used[v][i] == v
+            elif built[(m.dim, m.N, v)]:
+                assert (used[v][i] == v) == affine
         if built[(m.dim, m.N, 2)]:
             assert np.array_equal(runs[1][i], runs[2][i])
         if built[(m.dim, m.N, 0)]:
-            for v in (3, 4, 6, 7):
+            for v in B.PIPELINED:
                 if built[(m.dim, m.N, v)]:
                     assert np.array_equal(runs[0][i], runs[v][i])
+        if affine and built[(m.dim, m.N, 5)]:
+            for v in B.AFFINE:
+                if built[(m.dim, m.N, v)]:
+                    assert np.array_equal(runs[5][i], runs[v][i])
         assert max(relerr_fields(runs[0][i], runs[1][i])) < tol
+        if built[(m.dim, m.N, 5)]:
+            assert max(relerr_fields(runs[5][i], runs[1][i])) < tol_aff
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_shape_order_in_the_step_graph_does_not_change_results(cases, precision):
+    """Shapes as concurrent graph branches (default) or one after another:
+    every instance's arithmetic is the same, so the states are bit-identical."""
+    serial = _run_batch(cases, precision, concurrent=False)
+    conc = _run_batch(cases, precision)
+    for a, c in zip(serial, conc):
+        assert np.array_equal(a, c)
 
 
 def test_unbuilt_variant_is_rejected():

@@ -99,7 +99,7 @@ def test_batch_pipelined_variant(batch_cases, batch_refs):
 def test_batch_affine_even_orders(batch_cases, batch_refs):
     """The unwarped cube runs the affine stage (copies two groups ahead)."""
     for prec, tol in ((64, 1e-12), (32, 1e-5)):
-        out, used = _batch(batch_cases, prec, variant=0)
+        out, used = _batch(batch_cases, prec)  # the default variant: affine where it applies
         for (m, Q, dt, k), a, v, ref in zip(batch_cases, out, used, batch_refs):
             assert max(relerr_fields(a, ref)) < tol, (prec, m.N, m.nelem)
         assert used[-1] == B.VAR_AFFINE and all(v == 0 for v in used[:-1])
