@@ -437,13 +437,16 @@ class LSRK:
         check(_lib.lib().cb_solver_status_async(self._h, C.c_void_p(host.data_ptr())))
 
     def set_kernel(self, kernel: int) -> None:
-        """Stage kernel of the inviscid form: 0 = the shape's default, 1 = the
-        CUDA-core stages, 2 = the tensor-core (DMMA) stage of 3-D N=7 FP64."""
+        """Stage kernel: 0 = the shape's default, 1 = the CUDA-core stages,
+        2 = the tensor-core (DMMA) stage of the inviscid 3-D N=7 form, 3 = the
+        unpipelined grouped stages (for the fused viscous form: the grouped
+        stage pass instead of the pipelined one)."""
         check(_lib.lib().cb_solver_set_kernel(self._h, int(kernel)))
 
     @property
     def kernel(self) -> int:
-        """The stage kernel the solver runs: 1 CUDA-core, 2 tensor-core."""
+        """The stage kernel the solver runs: 1 CUDA-core, 2 tensor-core, 3
+        grouped."""
         v = C.c_int(0)
         check(_lib.lib().cb_solver_get_kernel(self._h, C.byref(v)))
         return v.value

@@ -227,7 +227,8 @@ cudaError_t b_prepare_visc(int sid) {
                                            (int)k.vsmem[pass][sid]);
       if (e != cudaSuccess) return e;
       int per_sm = 0;
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.vfn[pass][sid], BT, k.vsmem[pass][sid]);
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.vfn[pass][sid], k.vthreads[pass][sid],
+                                                        k.vsmem[pass][sid]);
       if (e != cudaSuccess) return e;
       k.vgrid[pass][sid] = num_sms() * std::max(per_sm, 1);
     }
@@ -405,9 +406,9 @@ cudaError_t build_graph(cb_batch *b, const std::bitset<NSHAPE> &shapes) {
     if (b->visc) {  // per stage: gradient pass, then the stage pass
       kp.func = (void *)K.vfn[pass][sid];
       kp.gridDim = dim3(K.vgrid[pass][sid]);
-      kp.blockDim = dim3(BT);
+      kp.blockDim = dim3(K.vthreads[pass][sid]);
       kp.sharedMemBytes = (unsigned)K.vsmem[pass][sid];
-      kp.kernelParams = gargs;
+      kp.kernelParams = K.vpipelined[pass][sid] ? pargs : gargs;
     } else {
       kp.func = (void *)K.fn[sid];
       kp.gridDim = dim3(K.grid[sid]);
@@ -567,6 +568,7 @@ int batch_add(cb_batch *b, const cb_mesh *m, void *Q, void *rhs, double dt, int6
   d.D = (const T *)m->D;
   d.nbr = m->nbr;
   d.status = b->status + slot;
+  d.gq = (T *)gq;
   d.start = b->steps;
   d.target = nsteps;
   d.dt = dt;

@@ -38,6 +38,7 @@ struct alignas(16) BDesc {
   const T *vgeo, *sgeo, *D;
   const int32_t *nbr;
   unsigned *status;  // the instance's status word
+  T *gq;             // gradient buffer (viscous batches)
   int64_t start, target;
   double dt;
   T qref[5];
@@ -723,6 +724,7 @@ struct BatchSrc {
   __device__ const T *sgeo(int it) const { return at(it).d.sgeo; }
   __device__ const int32_t *nbr(int it) const { return at(it).d.nbr; }
   __device__ const T *D(int it) const { return at(it).d.D; }
+  __device__ const T *gq(int it) const { return at(it).d.gq; }
   __device__ T qref(int it, int s) const { return at(it).d.qref[s]; }
   __device__ T rkbdt(int it) const { return T(rkb * at(it).d.dt); }
   __device__ unsigned *status(int it) const { return at(it).d.status; }
@@ -744,8 +746,9 @@ struct BKernels {
   bool pipelined[NSHAPE] = {}, ready[NSHAPE] = {};
   // viscous batches (variant 1 shapes only): gradient and stage passes
   const void *vfn[2][NSHAPE] = {};
-  int vgrid[2][NSHAPE] = {};
+  int vgrid[2][NSHAPE] = {}, vthreads[2][NSHAPE] = {};
   size_t vsmem[2][NSHAPE] = {};
+  bool vpipelined[2][NSHAPE] = {};  // the pass takes a BatchSrc (k_ns_stage_pipe)
   bool vready[NSHAPE] = {};
 };
 template <int DIM, int Nq, int G, typename T>
@@ -830,6 +833,17 @@ void b_fill(BKernels<T> &k) {
     k.vfn[1][id] = (const void *)k_ns_batch<DIM, Nq, T, false>;
     k.vsmem[0][id] = ns_smem<DIM, Nq, T>(0);
     k.vsmem[1][id] = ns_smem<DIM, Nq, T>(1);
+    k.vthreads[0][id] = k.vthreads[1][id] = BT;
+    // the pipelined stage pass where its plan fits (its groups have the
+    // element count of the grouped gradient pass: one work list serves both)
+    if constexpr (NsPipe<DIM, Nq, T>::OK) {
+      static_assert(Cfg<DIM, Nq>::EPB == BCfg<DIM, Nq, 0>::EPB, "one work list for both viscous passes");
+      using Src = BatchSrc<T, Lay<DIM>::NS, Cfg<DIM, Nq>::EPB, 3>;
+      k.vfn[1][id] = (const void *)k_ns_stage_pipe<DIM, Nq, T, Src>;
+      k.vsmem[1][id] = NsPipe<DIM, Nq, T>::smem() + Src::RING_BYTES;
+      k.vthreads[1][id] = Cfg<DIM, Nq>::THREADS;
+      k.vpipelined[1][id] = true;
+    }
   }
 }
 // Fill the table entries of one dimension (one translation unit per

@@ -759,6 +759,7 @@ __global__ void k_round_f32(float *__restrict__ dst, const double *__restrict__ 
 #include "cb_pipe.cuh"
 #include "cb_pipe2.cuh"
 #include "cb_mma.cuh"
+#include "cb_ns_pipe.cuh"
 namespace cb {
 
 // ---------------------------------------------------------------- launchers
@@ -823,7 +824,7 @@ struct Launch {
   // kernel: 0 = the default for the shape (the tensor-core stage where it is
   // built, else the pipelined CUDA-core stage, else the older ones), 1 = the
   // CUDA-core stages only, 2 = the tensor-core stage (cudaErrorNotSupported
-  // where it is not built).  probe != 0: the timeout test hook of the
+  // where it is not built), 3 = the unpipelined grouped stage k_stage.  probe != 0: the timeout test hook of the
   // pipelined stages (see MeshSrc); shapes without one return
   // cudaErrorNotSupported for it.
   // ebeg: the launch covers elements ebeg .. nelem - 1 (neighbour indices
@@ -855,7 +856,7 @@ struct Launch {
         return cudaGetLastError();
       }
     }
-    if (Pipe2<DIM, Nq, T>::OK && aligned2) {
+    if (Pipe2<DIM, Nq, T>::OK && aligned2 && kernel != 3) {
       using PP = Pipe2<DIM, Nq, T>;
       using S = MeshSrc<T, NS, C::EPB>;
       const size_t sm = PP::smem();
@@ -870,7 +871,7 @@ struct Launch {
       return cudaGetLastError();
     } else if (probe || ebeg) {
       return cudaErrorNotSupported;
-    } else if (pipe_ok && aligned) {
+    } else if (pipe_ok && aligned && kernel != 3) {
       using PP = Pipe<DIM, Nq, T>;
       size_t sm = PP::smem();
       cudaError_t err = prep(k_stage_pipe<DIM, Nq, T>, sm);

@@ -50,11 +50,11 @@ __device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes) {
 }
 
 // Shared-memory plan of the tensor-core stage (per block, one element per
-// group) for state, geometry and carry stored in T.  The flux planes are
-// FP64 in either case: the FP32 form (T = float) computes its fluxes in
-// FP32, contracts them with D on the FP64 tensor pipe (products of FP32
-// values are exact in FP64, the sums are rounded once) and rounds the
-// result to FP32.
+// group) for state, geometry, carry and flux planes stored in T.  The FP32
+// form (T = float) computes its fluxes in FP32, contracts them with D on the
+// FP64 tensor pipe (the FP32 plane values and D converted to FP64 as the
+// fragments are loaded: the products are exact, the sums are rounded once)
+// and rounds the result to FP32.
 template <typename T>
 struct PipeMT {
   static constexpr int DIM = 3, Nq = 8, Np = 512, Nfp = 64, NF = 6, NS = 5, NVG = 14, NSG = 5;
@@ -70,8 +70,8 @@ struct PipeMT {
   static constexpr int HP = 68, HS = 8 * HP;
   static constexpr size_t OFF_S = 16;
   static constexpr size_t OFF_FG = OFF_S + QB;
-  static constexpr size_t OFF_HZ = OFF_FG + sizeof(double) * WARPS * FGW;
-  static constexpr size_t OFF_FF = OFF_HZ + sizeof(double) * NS * HS;
+  static constexpr size_t OFF_HZ = OFF_FG + sizeof(T) * WARPS * FGW;
+  static constexpr size_t OFF_FF = OFF_HZ + sizeof(T) * NS * HS;
   static constexpr size_t FFB = sizeof(T) * NF * NS * Nfp;
   static constexpr size_t smem() { return OFF_FF + FFB; }  // item sources append their ring here
   // PFD = -1: each group's metric, carry and face geometry are prefetched
@@ -81,7 +81,9 @@ struct PipeMT {
   // (DRAM reads 1.17x / 1.62x the algorithmic bytes); same-group prefetch
   // reads 1.00x and is the fastest (127.6 us against 135 us without a
   // prefetch and 162 us for the CUDA-core stage).
-  static constexpr int MINB = 2, PFD = -1;
+  // FP32: the half-size plan (about 50 KB) leaves room for three blocks per
+  // SM if the registers fit 85 per thread
+  static constexpr int MINB = sizeof(T) == 8 ? 2 : 3, PFD = -1;
   // whether this stage is the default of its shape (the faster on B200 at
   // 32^3 hexes: FP64 0.974 ms per stage against 1.17 ms for the CUDA-core
   // stage, FP32 0.719 against 0.744 ms)
@@ -115,7 +117,7 @@ template <typename Src, int MINB = PipeM::MINB, int PFD = PipeM::PFD>
 __global__ void __launch_bounds__(PipeM::THREADS, MINB)
     k_stage_mma(Src src, PhysT<typename Src::Real> p, typename Src::Real rka) {
   using T = typename Src::Real;  // storage (and, for float, flux and update arithmetic)
-  using A = double;              // flux planes and tensor-core products
+  using A = double;              // tensor-core operands and products (planes stored in T)
   using V2 = typename Vec2<T>::type;
   using PM = PipeMT<T>;
   constexpr int DIM = 3, Nq = 8, Np = 512, Nfp = 64, NF = 6, NS = 5, NVG = 14, NSG = 5, IR = 3;
@@ -123,11 +125,11 @@ __global__ void __launch_bounds__(PipeM::THREADS, MINB)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   uint64_t *barS = reinterpret_cast<uint64_t *>(smem_raw);
   T *S = reinterpret_cast<T *>(smem_raw + PM::OFF_S);
-  A *FGall = reinterpret_cast<A *>(smem_raw + PM::OFF_FG);
-  A *HZ = reinterpret_cast<A *>(smem_raw + PM::OFF_HZ);
+  T *FGall = reinterpret_cast<T *>(smem_raw + PM::OFF_FG);
+  T *HZ = reinterpret_cast<T *>(smem_raw + PM::OFF_HZ);
   T *FF = reinterpret_cast<T *>(smem_raw + PM::OFF_FF);
   const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
-  A *FG = FGall + w * PM::FGW;
+  T *FG = FGall + w * PM::FGW;
   const int n0 = 2 * t + 8 * g + 64 * w;  // the lane's nodes n0, n0 + 1
 
   auto issue_S = [&](int it) {  // thread 0 only
@@ -285,8 +287,8 @@ __global__ void __launch_bounds__(PipeM::THREADS, MINB)
         for (int s = 0; s < NS; ++s) {
           T a = mt[r][0] * f[s][0] + mt[r][1] * f[s][1];
           a = a + mt[r][2] * f[s][2];
-          A *dst = r < 2 ? FG + (s * 2 + r) * 64 : HZ + s * PM::HS + w * PM::HP;
-          dst[pf] = A(MJ * a);
+          T *dst = r < 2 ? FG + (s * 2 + r) * 64 : HZ + s * PM::HS + w * PM::HP;
+          dst[pf] = MJ * a;
         }
       buoy[c] = MJ * q[IR] * p.grav;
     }
@@ -295,14 +297,14 @@ __global__ void __launch_bounds__(PipeM::THREADS, MINB)
     A acc[NS][2];
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
-      const A *Fp = FG + (s * 2 + 0) * 64, *Gp = FG + (s * 2 + 1) * 64;
+      const T *Fp = FG + (s * 2 + 0) * 64, *Gp = FG + (s * 2 + 1) * 64;
       A c0 = A(0), c1 = A(0);
       // xi: C[j][i] += Σ_m F[m, j]·D[m, i]   (A = F_kᵀ, B = D)
-      dmma(c0, c1, Fp[fg_pos(t, g)], Dg0, c0, c1);
-      dmma(c0, c1, Fp[fg_pos(t + 4, g)], Dg1, c0, c1);
+      dmma(c0, c1, A(Fp[fg_pos(t, g)]), Dg0, c0, c1);
+      dmma(c0, c1, A(Fp[fg_pos(t + 4, g)]), Dg1, c0, c1);
       // eta: C[j][i] += Σ_m D[m, j]·G[i, m]   (A = Dᵀ, B = G_k)
-      dmma(c0, c1, Dg0, Gp[fg_pos(g, t)], c0, c1);
-      dmma(c0, c1, Dg1, Gp[fg_pos(g, t + 4)], c0, c1);
+      dmma(c0, c1, Dg0, A(Gp[fg_pos(g, t)]), c0, c1);
+      dmma(c0, c1, Dg1, A(Gp[fg_pos(g, t + 4)]), c0, c1);
       acc[s][0] = c0;
       acc[s][1] = c1;
     }
@@ -324,14 +326,15 @@ __global__ void __launch_bounds__(PipeM::THREADS, MINB)
     // writes them over the H values it has just read (the same positions)
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
-      A *Hs = HZ + s * PM::HS;
+      T *Hs = HZ + s * PM::HS;
       const int pz = fg_pos(g, w);
-      const A a0 = Hs[t * PM::HP + pz], a1 = Hs[(t + 4) * PM::HP + pz];
+      const A a0 = A(Hs[t * PM::HP + pz]), a1 = A(Hs[(t + 4) * PM::HP + pz]);
       A z0 = A(0), z1 = A(0);
       dmma(z0, z1, a0, Dg0, z0, z1);
       dmma(z0, z1, a1, Dg1, z0, z1);
-      Hs[(2 * t) * PM::HP + pz] = z0;
-      Hs[(2 * t + 1) * PM::HP + pz] = z1;
+      // (FP32: rounded here instead of when added to R — the same rounding)
+      Hs[(2 * t) * PM::HP + pz] = T(z0);
+      Hs[(2 * t + 1) * PM::HP + pz] = T(z1);
     }
     // residual carry and 1/MJ of the lane's nodes
     V2 cr[NS];
@@ -349,14 +352,14 @@ __global__ void __launch_bounds__(PipeM::THREADS, MINB)
     for (int s = 0; s < NS; ++s) {
       // the lane's two zeta products: one 16-byte pair, in swapped order on
       // the rows whose column index is XOR-ed with 5
-      const double2 zp = *reinterpret_cast<const double2 *>(HZ + s * PM::HS + w * PM::HP + fg_pos(2 * t, g) - (((g >> 1) & 1)));
-      const double2 z = ((g >> 1) & 1) ? make_double2(zp.y, zp.x) : zp;
+      const V2 zp = *reinterpret_cast<const V2 *>(HZ + s * PM::HS + w * PM::HP + fg_pos(2 * t, g) - (((g >> 1) & 1)));
+      const V2 z = ((g >> 1) & 1) ? V2{zp.y, zp.x} : zp;
       T R[2] = {cr[s].x, cr[s].y};
 #pragma unroll
       for (int c = 0; c < 2; ++c) {
         if (s == DIM - 1) R[c] -= buoy[c];
         R[c] += T(acc[s][c]);
-        R[c] += T(c ? z.y : z.x);
+        R[c] += c ? z.y : z.x;
         const int i = 2 * t + c;
         if (i == 0) R[c] -= FF[(0 * NS + s) * Nfp + j + Nq * k];
         if (i == Nq - 1) R[c] -= FF[(1 * NS + s) * Nfp + j + Nq * k];

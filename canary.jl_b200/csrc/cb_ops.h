@@ -52,7 +52,9 @@ struct Ops {
                            cudaStream_t);
   // fused viscous passes over one mesh (pass 0: gradient, 1: stage + update);
   // nullptr for orders whose groups would need more than two nodes per thread
-  cudaError_t (*ns_pass)(int, const BDesc<T> &, T *, int64_t, const PhysT<T> &, T, T, cudaStream_t);
+  // pass 0 (gradient) or 1 (stage) of the fused viscous form; the last
+  // argument is the solver's kernel choice (3: the grouped stage pass)
+  cudaError_t (*ns_pass)(int, const BDesc<T> &, T *, int64_t, const PhysT<T> &, T, T, cudaStream_t, int);
 };
 
 // Defined in cb_inst_<dim>d_<prec>.cu; nullptr when N is outside 1..MAXN.

@@ -133,6 +133,7 @@ struct MeshSrc {
   // The launch covers elements ebeg_ .. nelem - 1 (a partitioned solve runs
   // the elements that read no ghost first, the others once ghosts arrived).
   int64_t ebeg_;
+  const T *gq_ = nullptr;  // gradient buffer (the viscous stage pass only)
   __device__ bool skip_copy(int it) const { return probe_ != 0 && it == 0; }
   __device__ uint32_t wait_limit() const { return probe_ ? PROBE_WAIT_LIMIT : WAIT_LIMIT; }
   __device__ void begin(unsigned char *) {}
@@ -155,6 +156,7 @@ struct MeshSrc {
   __device__ const T *sgeo(int) const { return sgeo_; }
   __device__ const int32_t *nbr(int) const { return nbr_; }
   __device__ const T *D(int) const { return D_; }
+  __device__ const T *gq(int) const { return gq_; }
   __device__ T qref(int, int s) const { return qref_.v[s]; }
   __device__ T rkbdt(int) const { return rkbdt_; }
   __device__ unsigned *status(int) const { return status_; }

@@ -93,8 +93,8 @@ cudaError_t enqueue_step(cb_solver *s, double dt, bool from_user) {
     for (int st = 0; st < 5 && e == cudaSuccess; ++st) {
       I.Q[0] = a;
       I.Q[1] = b;
-      if ((e = o->ns_pass(0, I, (T *)s->gradQ, s->nelem, p, T(0), T(0), s->stream)) != cudaSuccess) break;
-      e = o->ns_pass(1, I, (T *)s->gradQ, s->nelem, p, T(RKA[(st + 1) % 5]), T(RKB[st] * dt), s->stream);
+      if ((e = o->ns_pass(0, I, (T *)s->gradQ, s->nelem, p, T(0), T(0), s->stream, s->kernel)) != cudaSuccess) break;
+      e = o->ns_pass(1, I, (T *)s->gradQ, s->nelem, p, T(RKA[(st + 1) % 5]), T(RKB[st] * dt), s->stream, s->kernel);
       T *t = a;
       a = b;
       b = t;
@@ -199,8 +199,9 @@ cudaError_t enqueue_pass(cb_solver *s, int st, double dt, int pass) {
     I.status = s->status;
     I.dt = dt;
     for (int k = 0; k < 5; ++k) I.qref[k] = T(s->qref[k]);
-    return pass == 0 ? o->ns_pass(0, I, (T *)s->gradQ, s->nelem, p, T(0), T(0), s->stream)
-                     : o->ns_pass(1, I, (T *)s->gradQ, s->nelem, p, T(RKA[(st + 1) % 5]), T(RKB[st] * dt), s->stream);
+    return pass == 0 ? o->ns_pass(0, I, (T *)s->gradQ, s->nelem, p, T(0), T(0), s->stream, s->kernel)
+                     : o->ns_pass(1, I, (T *)s->gradQ, s->nelem, p, T(RKA[(st + 1) % 5]), T(RKB[st] * dt), s->stream,
+                                  s->kernel);
   }
   if (pass == 0) return cudaSuccess;
   Offs<T, 5> q5;
@@ -602,12 +603,12 @@ int cb_solver_set_offset(cb_solver *s, const double *qref) {
 }
 
 int cb_solver_set_kernel(cb_solver *s, int kernel) {
-  if (!s || kernel < 0 || kernel > 2) return solver_fail(CB_ERR_ARG, "cb_solver_set_kernel: bad arguments");
+  if (!s || kernel < 0 || kernel > 3) return solver_fail(CB_ERR_ARG, "cb_solver_set_kernel: bad arguments");
   if (kernel == 2) {
     const bool mma = s->prec == 64 ? ops<double>(s)->mma : ops<float>(s)->mma;
     if (!mma || s->phys.visc > 0)
       return solver_fail(CB_ERR_UNSUPPORTED,
-                         "cb_solver_set_kernel: the tensor-core stage is built for the inviscid 3-D N=7 FP64 form");
+                         "cb_solver_set_kernel: the tensor-core stage is built for the inviscid 3-D N=7 form");
   }
   if (kernel != s->kernel) drop_graph(s);
   s->kernel = kernel;

@@ -184,15 +184,16 @@ int cb_solver_sums(cb_solver *s, double *out_host);
  * non-finite state) into *out_host (page-locked memory for an asynchronous
  * copy); the value is valid once the stream has reached the copy. */
 int cb_solver_status_async(cb_solver *s, unsigned *out_host);
-/* Stage kernel of the inviscid form: 0 = the default for the shape, 1 = the
- * CUDA-core stages (pipelined bulk-copy staging where the plan fits), 2 = the
- * tensor-core stage (D contraction on the FP64 tensor pipe as 8x8x4 DMMA
- * tiles, for FP32 solvers on the FP32 fluxes converted to FP64, the sum
- * rounded once; built for 3-D N=7, CB_ERR_UNSUPPORTED elsewhere).  The
- * default is whichever of the two is faster on B200 for the shape.  Both agree with
- * the oracle to round-off; changing it re-captures the step graph at the
- * next run.
- * cb_solver_get_kernel reports the kernel the solver runs (1 or 2). */
+/* Stage kernel: 0 = the default for the shape, 1 = the CUDA-core stages
+ * (pipelined bulk-copy staging where the plan fits), 2 = the tensor-core
+ * stage of the inviscid form (D contraction on the FP64 tensor pipe as 8x8x4
+ * DMMA tiles, for FP32 solvers on the FP32 fluxes converted to FP64, the sum
+ * rounded once; built for 3-D N=7, CB_ERR_UNSUPPORTED elsewhere), 3 = the
+ * unpipelined grouped stages (the inviscid k_stage; for the fused viscous
+ * form the grouped stage pass instead of the pipelined one).  The default is
+ * the fastest on B200 for the shape.  All agree with the oracle to
+ * round-off; changing it re-captures the step graph at the next run.
+ * cb_solver_get_kernel reports the kernel the solver runs (1, 2 or 3). */
 int cb_solver_set_kernel(cb_solver *s, int kernel);
 int cb_solver_get_kernel(const cb_solver *s, int *kernel);
 /* Clear the solver's sticky status bits (stream-ordered). */

@@ -310,6 +310,33 @@ def test_viscous_solver_3d(N, walls):
         s.close()
 
 
+@pytest.mark.parametrize("dim,N,walls", [(3, 3, True), (3, 4, False), (3, 5, True), (3, 7, False), (2, 4, True),
+                                         (2, 7, False)])
+def test_pipelined_viscous_stage_pass(dim, N, walls):
+    """The fused viscous form with the pipelined stage pass (k_ns_stage_pipe:
+    bulk-copied state and gradient slabs, the default) and with the grouped
+    one (kernel 3): both against the oracle at 1e-12 relative L2 per field,
+    and each other to round-off (1e-13); 3-D even orders take the ragged
+    16-byte-rounded slab copies."""
+    m = make_mesh(dim, N, n=3 if dim == 3 else 5, periodic=not walls)
+    ph = dict(dg.WORKLOAD_PHYS, visc=0.02)
+    Q = random_state(m, 21 + N)
+    dt, k = 2e-4, 3
+    ref, rref = Q.copy(order="F"), np.zeros_like(Q, order="F")
+    O.lowstorageRK(dim, N, m.vgeo, m.sgeo, ref, rref, m.D, dt, k, m.vmapM, m.vmapP, m.elemtobndy,
+                   oracle_phys(ph), NT)
+    dm = dg.DeviceMesh.upload(m)
+    out = {}
+    for kernel in (0, 3):
+        s = dg.LSRK.for_state(dm, Q, 64, phys=dg.make_phys(**ph))
+        s.set_kernel(kernel)
+        s.run(k, dt)
+        out[kernel] = s.state()
+        s.close()
+        assert relerr(out[kernel], ref) < 1e-12, kernel
+    assert relerr(out[0], out[3]) < 1e-13
+
+
 def test_invalid_boundary_code_is_reported():
     import torch
     from canary_b200._lib import CanaryError, CB_ERR_BC
