@@ -374,7 +374,8 @@ def batched_ensemble(count=512, seed=0, steps=500, device="cuda", parity_sample=
                             report=rep) if tune else {}
         out[f"autotune_fp{prec}_s"] = round(time.time() - t1, 2)
         out[f"autotune_fp{prec}"] = {f"{d},{n}": {"variant": r["variant"], **r["config"],
-                                                   "instances": r["instances"], "nodes": r["nodes"],
+                                                   "instances": r["instances"], "admitted": r["admitted"],
+                                                   "nodes": r["nodes"],
                                                    "ms_per_step": {str(v): round(t, 4) for v, t in r["ms_per_step"].items()}}
                                      for (d, n), r in rep.items()}
         ens = B.VortexEnsemble(params, prec, nsteps=steps, cache=cache, tuning=tuning)

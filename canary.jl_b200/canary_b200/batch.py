@@ -341,7 +341,7 @@ def _time_variants(precision, dim, N, meshes, steps, repeat, affine):
     return timings
 
 
-def autotune(precision: int, shapes, nodes_target: int = 4_000_000, steps: int = 4, repeat: int = 3,
+def autotune(precision: int, shapes, nodes_target: int = 8_000_000, steps: int = 4, repeat: int = 3,
              stream=None, instances=None, report=None, affine=None) -> dict:
     """Choose the stage variant of each (dim, N) — pipelined staging at one of
     several occupancies, two element groups ahead, twice the elements per
@@ -353,7 +353,9 @@ def autotune(precision: int, shapes, nodes_target: int = 4_000_000, steps: int =
 
     With `instances` (the workload's (dim, N, n_side) list) each shape is
     timed on the workload's own instances of that shape, taken in order up to
-    about `nodes_target` nodes (its actual size mix); otherwise on one
+    about `nodes_target` nodes (its actual size mix) and repeated in the same
+    order while they hold fewer — so that the timed state does not stay in
+    L2 between stages, as it does not in the whole workload; otherwise on one
     synthetic instance of about `nodes_target` nodes: the 2-D vortex / the
     3-D Fourier state on periodic meshes built on the device.  Returns
     {(dim, N): variant}; `report` (a dict) receives, per shape, the timings
@@ -371,6 +373,13 @@ def autotune(precision: int, shapes, nodes_target: int = 4_000_000, steps: int =
                 if (d, n) == (dim, N) and nodes < nodes_target:
                     picks.append(ns)
                     nodes += ns ** dim * (N + 1) ** dim
+            distinct = len(picks)
+            k = 0
+            while picks and nodes < nodes_target:  # the same instances again, in order
+                ns = picks[k % distinct]
+                picks.append(ns)
+                nodes += ns ** dim * (N + 1) ** dim
+                k += 1
             dms = {}
             meshes = []
             real = torch.float64 if precision == 64 else torch.float32
@@ -394,7 +403,8 @@ def autotune(precision: int, shapes, nodes_target: int = 4_000_000, steps: int =
             best[(dim, N)] = min(timings, key=timings.get)
             if report is not None:
                 info = Batch(precision, 1)
-                report[(dim, N)] = {"variant": best[(dim, N)], "instances": len(picks), "nodes": nodes,
+                report[(dim, N)] = {"variant": best[(dim, N)], "instances": distinct, "admitted": len(picks),
+                                    "nodes": nodes,
                                     "ms_per_step": timings,
                                     "config": info.variant_info(dim, N, best[(dim, N)])}
                 info.close()

@@ -834,13 +834,19 @@ void b_fill(BKernels<T> &k) {
     k.vsmem[0][id] = ns_smem<DIM, Nq, T>(0);
     k.vsmem[1][id] = ns_smem<DIM, Nq, T>(1);
     k.vthreads[0][id] = k.vthreads[1][id] = BT;
-    // the pipelined stage pass where its plan fits (its groups have the
-    // element count of the grouped gradient pass: one work list serves both)
+    // the pipelined passes where their plans fit (their groups have the
+    // element count of the grouped passes: one work list serves all)
+    static_assert(Cfg<DIM, Nq>::EPB == BCfg<DIM, Nq, 0>::EPB, "one work list for both viscous passes");
+    using VSrc = BatchSrc<T, Lay<DIM>::NS, Cfg<DIM, Nq>::EPB, 3>;
+    if constexpr (NsGradPipe<DIM, Nq, T>::OK) {
+      k.vfn[0][id] = (const void *)k_ns_grad_pipe<DIM, Nq, T, VSrc>;
+      k.vsmem[0][id] = NsGradPipe<DIM, Nq, T>::smem() + VSrc::RING_BYTES;
+      k.vthreads[0][id] = Cfg<DIM, Nq>::THREADS;
+      k.vpipelined[0][id] = true;
+    }
     if constexpr (NsPipe<DIM, Nq, T>::OK) {
-      static_assert(Cfg<DIM, Nq>::EPB == BCfg<DIM, Nq, 0>::EPB, "one work list for both viscous passes");
-      using Src = BatchSrc<T, Lay<DIM>::NS, Cfg<DIM, Nq>::EPB, 3>;
-      k.vfn[1][id] = (const void *)k_ns_stage_pipe<DIM, Nq, T, Src>;
-      k.vsmem[1][id] = NsPipe<DIM, Nq, T>::smem() + Src::RING_BYTES;
+      k.vfn[1][id] = (const void *)k_ns_stage_pipe<DIM, Nq, T, VSrc>;
+      k.vsmem[1][id] = NsPipe<DIM, Nq, T>::smem() + VSrc::RING_BYTES;
       k.vthreads[1][id] = Cfg<DIM, Nq>::THREADS;
       k.vpipelined[1][id] = true;
     }

@@ -367,4 +367,256 @@ k_ns_stage_pipe(Src src, PhysT<T> p, T rka) {
   }
 }
 
+// Gradient pass on the same schedule (k_ns_grad_pipe): the group's state
+// slab by bulk copy one group ahead, metric and face geometry from L2
+// (prefetched at the top of the group's iteration), the primitives' face
+// averages for every gradient component computed once, then per component
+// the flux rows MJ ξ_r,c prim, the contraction with Dᵀ (subtracted), the face
+// terms in face order and ×MJI into gQ — ns_grad_group's arithmetic.
+template <int DIM, int Nq, typename T>
+struct NsGradPipe {
+  using C = Cfg<DIM, Nq>;
+  using P1 = Pipe<DIM, Nq, T>;
+  using PS = NsPipe<DIM, Nq, T>;
+  static constexpr int NS = Lay<DIM>::NS, ND = NS * DIM;
+  static constexpr size_t pad16(size_t b) { return (b + 15) & ~size_t(15); }
+  static constexpr size_t OFF_D = 16;
+  static constexpr size_t OFF_S = OFF_D + pad16(sizeof(T) * Nq * P1::RS);
+  static constexpr size_t OFF_F = OFF_S + PS::QS;
+  static constexpr size_t OFF_FF = OFF_F + pad16(sizeof(T) * DIM * P1::FDIR);
+  static constexpr size_t FFB = sizeof(T) * (size_t)C::NFACE * ND * C::EPB * C::Nfp;
+  static constexpr size_t smem() { return OFF_FF + pad16(FFB); }  // sources append their ring here
+  static constexpr int MINB = PS::MINB;
+  static constexpr bool OK = MINB * (smem() + PS::RING_MAX + 1024) <= 228 * 1024 && smem() + PS::RING_MAX <= SMEM_LIMIT;
+};
+
+template <int DIM, int Nq, typename T, typename Src, int MINB = NsGradPipe<DIM, Nq, T>::MINB>
+__global__ void __launch_bounds__(Cfg<DIM, Nq>::THREADS, MINB)
+k_ns_grad_pipe(Src src, PhysT<T> p, T) {
+  using C = Cfg<DIM, Nq>;
+  using PP = NsGradPipe<DIM, Nq, T>;
+  using PS = NsPipe<DIM, Nq, T>;
+  static_assert(Src::AHEAD >= 1, "the source must publish the next group before the top of an iteration");
+  constexpr int NS = Lay<DIM>::NS, NVG = Lay<DIM>::NVG, NSG = Lay<DIM>::NSG, IR = Lay<DIM>::IR, IE = Lay<DIM>::IE;
+  constexpr int Np = C::Np, Nfp = C::Nfp, NF = C::NFACE, EPB = C::EPB, SP = C::SLOTS, ND = NS * DIM;
+  constexpr int MJF = DIM * DIM, MJIF = DIM * DIM + 1, GC = DIM * DIM + 2 + DIM - 1;
+  constexpr int FS = EPB * Nfp, RS = PS::RS, NR = PS::NR;
+  constexpr int64_t SE = (int64_t)NSG * Nfp * NF;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw);
+  T *DT = reinterpret_cast<T *>(smem_raw + PP::OFF_D);
+  T *Sq0 = reinterpret_cast<T *>(smem_raw + PP::OFF_S);  // [EPB][NS][Np] state
+  T *sF = reinterpret_cast<T *>(smem_raw + PP::OFF_F);   // flux rows of one gradient component
+  T *FF = reinterpret_cast<T *>(smem_raw + PP::OFF_FF);  // [NF][NS*DIM][FS] face terms
+  const int tid = threadIdx.x;
+
+  auto head_of = [](const T *g) -> uint32_t {
+    return PS::RAG ? (uint32_t)(reinterpret_cast<uintptr_t>(g) & 15) : 0u;
+  };
+  auto issue = [&](int it) {  // thread 0 only: the group's state slab (see NsPipe::RAG)
+    if (src.skip_copy(it)) return;
+    const int64_t e0 = src.e0(it);
+    const int nv = src.nv(it);
+    const bool last = PS::RAG && src.last(it);
+    const T *q = src.Qin(it) + e0 * Np * NS;
+    const uint32_t head = head_of(q);
+    const uint32_t end = head + (uint32_t)(nv * PS::QB);
+    const uint32_t L = PS::RAG ? (last ? (end & ~15u) : ((end + 15u) & ~15u)) : end;
+    const unsigned char *base = reinterpret_cast<const unsigned char *>(q) - head;
+    if (last)  // the last (< 16) bytes of the array by plain loads
+      for (uint32_t b = L > head ? L : head; b < end; b += sizeof(T))
+        *reinterpret_cast<T *>(reinterpret_cast<unsigned char *>(Sq0) + b) = *reinterpret_cast<const T *>(base + b);
+    fence_proxy_async();
+    mbar_expect_tx(bar, L);
+    if (L) bulk_g2s(Sq0, base, L, bar);
+  };
+
+  src.begin(smem_raw + PP::smem());
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    fence_mbar_init();
+  }
+  if constexpr (PS::MV > Nq)
+    for (size_t t = tid; t < (size_t)DIM * PS::FDIR; t += C::THREADS)
+      if ((int)(t % RS) >= Nq) sF[t] = T(0);
+  __syncthreads();
+  if (tid == 0 && src.valid(0)) issue(0);
+
+  int32_t nbn[C::FPT];
+  auto load_nbr = [&](int it, int32_t *dst) {
+    const bool ok = src.valid(it);
+    const int64_t e0 = ok ? src.e0(it) : 0;
+    const int nv = ok ? src.nv(it) : 0;
+    const int32_t *nb = src.nbr(it);
+#pragma unroll
+    for (int u = 0; u < C::FPT; ++u) {
+      const int fs = tid + u * C::THREADS;
+      const int el = fs / (NF * Nfp), f = (fs / Nfp) % NF;
+      dst[u] = (fs < C::FSLOTS && el < nv) ? nb[f + NF * (e0 + el)] : NBR_WALL;
+    }
+  };
+  load_nbr(0, nbn);
+
+  bool timed_out = false;
+  const T *curD = nullptr;
+  for (int it = 0; src.valid(it); ++it) {
+    const int64_t e0 = src.e0(it);
+    const int nv = src.nv(it);
+    const bool more = src.valid(it + 1);
+    if (tid == Src::PUBLISHER) src.prefetch();
+    const T *__restrict__ Qin = src.Qin(it);
+    const T *__restrict__ vgeo = src.vgeo(it);
+    const T *__restrict__ vg = vgeo + e0 * Np * NVG;
+    const T *__restrict__ sg = src.sgeo(it) + e0 * SE;
+    T *__restrict__ gq = const_cast<T *>(src.gq(it)) + e0 * Np * NS * DIM;
+    for (int el = 0; el < nv; ++el) prefetch_lines_l2(vg + el * Np * NVG, sizeof(T) * Np * (MJIF + 1));
+    prefetch_lines_l2(sg, sizeof(T) * nv * SE);
+    T qr[NS];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) qr[s] = src.qref(it, s);
+    int32_t nbv[C::FPT];
+#pragma unroll
+    for (int u = 0; u < C::FPT; ++u) nbv[u] = nbn[u];
+    load_nbr(it + 1, nbn);
+
+    if (!mbar_wait_bounded(bar, (uint32_t)(it & 1), src.wait_limit())) timed_out = true;
+    const T *Sq = Sq0 + head_of(Qin + e0 * Np * NS) / sizeof(T);
+    if (src.D(it) != curD) {  // read after the first component's barrier
+      curD = src.D(it);
+      for (int t = tid; t < Nq * RS; t += C::THREADS) {
+        const int i = t / RS, m = t % RS;
+        DT[t] = m < Nq ? curD[m + Nq * i] : T(0);
+      }
+    }
+
+    // ---- primitives of the thread's nodes, metric kept in registers
+    T prim[C::NPT][NS], met[C::NPT][DIM][DIM], MJ[C::NPT], mji[C::NPT];
+#pragma unroll
+    for (int u = 0; u < C::NPT; ++u) {
+      const int slot = tid + u * C::THREADS;
+      const int el = slot / Np, n = slot % Np;
+      if (slot < SP && el < nv) {
+        T q[NS];
+#pragma unroll
+        for (int s = 0; s < NS; ++s) q[s] = Sq[(el * NS + s) * Np + n] + qr[s];
+        const T *G = vg + (int64_t)el * Np * NVG;
+#pragma unroll
+        for (int r = 0; r < DIM; ++r)
+#pragma unroll
+          for (int c = 0; c < DIM; ++c) met[u][r][c] = G[(r + DIM * c) * Np + n];
+        MJ[u] = G[MJF * Np + n];
+        mji[u] = G[MJIF * Np + n];
+        const T gc = p.grav != T(0) ? G[GC * Np + n] : T(0);
+        primitives<DIM, T>(q, gc, p, prim[u]);
+      }
+    }
+    // ---- face averages of the primitives (flux_grad!) for every component
+#pragma unroll
+    for (int u = 0; u < C::FPT; ++u) {
+      const int fs = tid + u * C::THREADS;
+      const int el = fs / (NF * Nfp), f = (fs / Nfp) % NF, fn = fs % Nfp;
+      if (fs < C::FSLOTS && el < nv) {
+        const int vM = face_node<DIM, Nq>(f, fn);
+        const T *sgp = sg + NSG * (fn + Nfp * (f + NF * el));
+        T nrm[DIM];
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) nrm[c] = sgp[c];
+        const T sMJ = sgp[DIM];
+        T qM[NS], pM[NS], pP[NS];
+#pragma unroll
+        for (int s = 0; s < NS; ++s) qM[s] = Sq[(el * NS + s) * Np + vM] + qr[s];
+        const T gM = p.grav != T(0) ? vg[vM + Np * (GC + (int64_t)NVG * el)] : T(0);
+        primitives<DIM, T>(qM, gM, p, pM);
+        const int32_t nb = nbv[u];
+        if (nb >= 0) {
+          const int64_t e2 = nb >> 3;
+          const int vP = face_node<DIM, Nq>(nb & 7, fn);
+          T qP[NS];
+#pragma unroll
+          for (int s = 0; s < NS; ++s) qP[s] = Qin[vP + Np * (s + NS * e2)] + qr[s];
+          const T gP = p.grav != T(0) ? vgeo[vP + Np * (GC + NVG * e2)] : T(0);
+          primitives<DIM, T>(qP, gP, p, pP);
+        } else {  // reflective wall: mirrored velocity, same density and temperature
+          T qP[NS];
+          wall_state<DIM, T>(qM, nrm, qP);
+#pragma unroll
+          for (int c = 0; c < DIM; ++c) pP[c] = qP[c] / qM[IR];
+          pP[IR] = qM[IR];
+          pP[IE] = pM[IE];
+        }
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+          const T fsv = T(0.5) * (pM[s] + pP[s]);
+#pragma unroll
+          for (int c = 0; c < DIM; ++c) FF[(f * ND + s * DIM + c) * FS + el * Nfp + fn] = sMJ * nrm[c] * fsv;
+        }
+      }
+    }
+    // ---- per gradient component: flux rows, contraction (subtracted), face
+    // terms in face order, ×MJI into gQ (unrolled: the metric column is
+    // chosen at compile time, not by indexing a register array)
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+#pragma unroll
+      for (int u = 0; u < C::NPT; ++u) {
+        const int slot = tid + u * C::THREADS;
+        const int el = slot / Np, n = slot % Np;
+        if (slot < SP && el < nv) {
+          const int i = n % Nq, j = (n / Nq) % Nq, k = DIM == 3 ? n / (Nq * Nq) : 0;
+#pragma unroll
+          for (int r = 0; r < DIM; ++r) {
+            const int row = DIM == 2 ? (r == 0 ? j : i) : (r == 0 ? j + Nq * k : (r == 1 ? i + Nq * k : i + Nq * j));
+            const int pos = r == 0 ? i : (r == 1 ? j : k);
+#pragma unroll
+            for (int s = 0; s < NS; ++s)
+              sF[r * PS::FDIR + ((size_t)(s * EPB + el) * NR + row) * RS + pos] = MJ[u] * (met[u][r][c] * prim[u][s]);
+          }
+        }
+      }
+      if (c == 0) {
+        // first barrier of the group: FF and the first rows are complete, the
+        // state slab is no longer read; agree on a wait that gave up
+        if (__syncthreads_or(timed_out)) {
+          if (tid == 0) {
+            atomicOr(src.status(it), ST_TIMEOUT);
+            mbar_wait_bounded(bar, (uint32_t)(it & 1), src.wait_limit());
+          }
+          return;
+        }
+        if (tid == 0 && more) issue(it + 1);
+        if ((tid >> 5) == (Src::PUBLISHER >> 5)) src.publish(it);
+      } else {
+        __syncthreads();
+      }
+#pragma unroll
+      for (int u = 0; u < C::NPT; ++u) {
+        const int slot = tid + u * C::THREADS;
+        const int el = slot / Np, n = slot % Np;
+        if (slot < SP && el < nv) {
+          T R[NS];
+#pragma unroll
+          for (int s = 0; s < NS; ++s) R[s] = T(0);
+          contract_rows<DIM, Nq, T>(sF, DT, el, n, R);
+#pragma unroll
+          for (int s = 0; s < NS; ++s) R[s] = -R[s];
+          const int i = n % Nq, j = (n / Nq) % Nq, k = DIM == 3 ? n / (Nq * Nq) : 0;
+          auto add = [&](int f, int fn) {
+#pragma unroll
+            for (int s = 0; s < NS; ++s) R[s] += FF[(f * ND + s * DIM + c) * FS + el * Nfp + fn];
+          };
+          if (i == 0) add(0, DIM == 3 ? j + Nq * k : j);
+          if (i == Nq - 1) add(1, DIM == 3 ? j + Nq * k : j);
+          if (j == 0) add(2, DIM == 3 ? i + Nq * k : i);
+          if (j == Nq - 1) add(3, DIM == 3 ? i + Nq * k : i);
+          if (DIM == 3 && k == 0) add(4, i + Nq * j);
+          if (DIM == 3 && k == Nq - 1) add(5, i + Nq * j);
+#pragma unroll
+          for (int s = 0; s < NS; ++s) gq[n + Np * (s + NS * (c + (int64_t)DIM * el))] = R[s] * mji[u];
+        }
+      }
+      __syncthreads();  // the rows are rewritten for the next component (the last: FF and the ring are free)
+    }
+  }
+}
+
 }  // namespace cb

@@ -312,12 +312,12 @@ def test_viscous_solver_3d(N, walls):
 
 @pytest.mark.parametrize("dim,N,walls", [(3, 3, True), (3, 4, False), (3, 5, True), (3, 7, False), (2, 4, True),
                                          (2, 7, False)])
-def test_pipelined_viscous_stage_pass(dim, N, walls):
-    """The fused viscous form with the pipelined stage pass (k_ns_stage_pipe:
-    bulk-copied state and gradient slabs, the default) and with the grouped
-    one (kernel 3): both against the oracle at 1e-12 relative L2 per field,
-    and each other to round-off (1e-13); 3-D even orders take the ragged
-    16-byte-rounded slab copies."""
+def test_pipelined_viscous_passes(dim, N, walls):
+    """The fused viscous form with the pipelined passes (k_ns_grad_pipe and
+    k_ns_stage_pipe: bulk-copied state (and gradient) slabs, the default) and
+    with the grouped ones (kernel 3): both against the oracle at 1e-12
+    relative L2 per field, and each other to round-off (1e-13); 3-D even
+    orders take the ragged 16-byte-rounded slab copies."""
     m = make_mesh(dim, N, n=3 if dim == 3 else 5, periodic=not walls)
     ph = dict(dg.WORKLOAD_PHYS, visc=0.02)
     Q = random_state(m, 21 + N)
