@@ -515,7 +515,7 @@ def main():
                     help="stage kernel: 0 default, 1 CUDA-core pipelined, 2 tensor-core (3-D N=7 FP64)")
     ap.add_argument("--ref-n-side", type=int, default=None,
                     help="mesh of the reference arm (default: --n-side, the same workload)")
-    ap.add_argument("--e2e-steps", type=int, default=8)
+    ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--parity-steps", type=int, default=200,
                     help="steps of the full-size parity run against the oracle (0: skip)")
     ap.add_argument("--precision-steps", type=int, default=1000,
