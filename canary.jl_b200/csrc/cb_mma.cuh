@@ -84,7 +84,8 @@ struct PipeMT {
   // FP32: the half-size plan (about 50 KB) leaves room for three blocks per
   // SM if the registers fit 85 per thread (measured at 32^3: 0.566 ms per
   // stage; four blocks at 64 registers spill and take 0.637 ms)
-  static constexpr int MINB = sizeof(T) == 8 ? 2 : 3, PFD = sizeof(T) == 8 ? -1 : 1;
+  // (FP32 with the prefetch one group ahead: 0.567 ms, the same)
+  static constexpr int MINB = sizeof(T) == 8 ? 2 : 3, PFD = -1;
   // whether this stage is the default of its shape (the faster on B200 at
   // 32^3 hexes: FP64 0.974 ms per stage against 1.17 ms for the CUDA-core
   // stage, FP32 0.719 against 0.744 ms)
