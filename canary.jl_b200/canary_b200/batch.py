@@ -341,6 +341,26 @@ def _time_variants(precision, dim, N, meshes, steps, repeat, affine):
     return timings
 
 
+def tuning_picks(instances, dim: int, N: int, nodes_target: int):
+    """The instances the tuner times for (dim, N): the workload's own
+    (n_side of each (dim, N, n_side) entry of that shape), in order, up to
+    about `nodes_target` nodes, then the same ones again in order while they
+    hold fewer.  Returns (n_side list, distinct workload instances, nodes)."""
+    picks, nodes = [], 0
+    for d, n, ns in instances:
+        if (d, n) == (dim, N) and nodes < nodes_target:
+            picks.append(ns)
+            nodes += ns ** dim * (N + 1) ** dim
+    distinct = len(picks)
+    k = 0
+    while picks and nodes < nodes_target:  # the same instances again, in order
+        ns = picks[k % distinct]
+        picks.append(ns)
+        nodes += ns ** dim * (N + 1) ** dim
+        k += 1
+    return picks, distinct, nodes
+
+
 def autotune(precision: int, shapes, nodes_target: int = 8_000_000, steps: int = 4, repeat: int = 3,
              stream=None, instances=None, report=None, affine=None) -> dict:
     """Choose the stage variant of each (dim, N) — pipelined staging at one of
@@ -368,18 +388,7 @@ def autotune(precision: int, shapes, nodes_target: int = 8_000_000, steps: int =
     if instances is not None:
         for dim, N in shapes:
             L = 10.0 if dim == 2 else 2 * np.pi
-            picks, nodes = [], 0
-            for d, n, ns in instances:
-                if (d, n) == (dim, N) and nodes < nodes_target:
-                    picks.append(ns)
-                    nodes += ns ** dim * (N + 1) ** dim
-            distinct = len(picks)
-            k = 0
-            while picks and nodes < nodes_target:  # the same instances again, in order
-                ns = picks[k % distinct]
-                picks.append(ns)
-                nodes += ns ** dim * (N + 1) ** dim
-                k += 1
+            picks, distinct, nodes = tuning_picks(instances, dim, N, nodes_target)
             dms = {}
             meshes = []
             real = torch.float64 if precision == 64 else torch.float32
