@@ -217,6 +217,15 @@ __global__ void __launch_bounds__(PipeM::THREADS, MINB)
         }
       }
     }
+    // the lane's metric (+ MJ): FP32 loads it here, so that its latency
+    // overlaps the wait for the state slab and the face phase (FP64 waits
+    // until after the face phase, whose registers it would crowd: 100 bytes
+    // of spill at 128 registers)
+    V2 met[DIM * DIM + 1];
+    if constexpr (sizeof(T) == 4) {
+#pragma unroll
+      for (int f = 0; f <= MJF; ++f) met[f] = *reinterpret_cast<const V2 *>(vg + n0 + Np * f);
+    }
     if (!mbar_wait_bounded(&barS[0], (uint32_t)(it & 1), src.wait_limit())) timed_out = true;
 
     // ---- face fluxes (any thread, any face node) into FF
@@ -256,11 +265,11 @@ __global__ void __launch_bounds__(PipeM::THREADS, MINB)
     }
 
     // ---- volume fluxes of the lane's two nodes, one node at a time: F, G
-    // into the warp's planes, H into the shared zeta buffer (the metric is
-    // loaded here, after the face phase, whose registers it would crowd)
-    V2 met[DIM * DIM + 1];
+    // into the warp's planes, H into the shared zeta buffer
+    if constexpr (sizeof(T) == 8) {
 #pragma unroll
-    for (int f = 0; f <= MJF; ++f) met[f] = *reinterpret_cast<const V2 *>(vg + n0 + Np * f);
+      for (int f = 0; f <= MJF; ++f) met[f] = *reinterpret_cast<const V2 *>(vg + n0 + Np * f);
+    }
     T qd[2][NS], buoy[2];
 #pragma unroll
     for (int c = 0; c < 2; ++c) {
