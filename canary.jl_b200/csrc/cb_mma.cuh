@@ -22,6 +22,10 @@
 //     is read from shared memory once per direction (one 8-byte fragment
 //     element), instead of a whole row per node as in the CUDA-core
 //     contraction;
+//   * the neighbours' state traces of each face slot are loaded into
+//     registers before the wait for the state slab (FP64), or copied into
+//     shared memory one group ahead by the thread that owns the slot
+//     (cp.async, issued as soon as it has used the current ones; FP32);
 //   * only the state (read by the face phase for other threads' nodes) is
 //     staged in shared memory, by a bulk copy one group ahead; the metric,
 //     the residual carry and the face geometry are each read by the one
@@ -73,7 +77,16 @@ struct PipeMT {
   static constexpr size_t OFF_HZ = OFF_FG + sizeof(T) * WARPS * FGW;
   static constexpr size_t OFF_FF = OFF_HZ + sizeof(T) * NS * HS;
   static constexpr size_t FFB = sizeof(T) * NF * NS * Nfp;
-  static constexpr size_t smem() { return OFF_FF + FFB; }  // item sources append their ring here
+  // FP32: neighbour state traces of each face slot, [NS][FSLOTS]: every
+  // thread copies its own slots' traces of the next group asynchronously
+  // (cp.async) once it has used this group's, and reads them only itself.
+  // FP64 loads them into registers at the top of the group instead: with
+  // the 15 KB buffer its two blocks leave 28 KB of L1 per SM and the stage
+  // took 1.13 ms instead of 0.98 at 32^3; FP32 went from 0.530 to 0.519 ms.
+  static constexpr bool ASYNC_QP = sizeof(T) == 4;
+  static constexpr size_t OFF_QP = OFF_FF + FFB;
+  static constexpr size_t QPB = ASYNC_QP ? sizeof(T) * NS * FSLOTS : 0;
+  static constexpr size_t smem() { return OFF_QP + QPB; }  // item sources append their ring here
   // PFD = -1: each group's metric, carry and face geometry are prefetched
   // into L2 at the top of its own iteration.  Measured on B200 (16^3-hex
   // launch, ncu): prefetching one or two groups ahead lets the streaming
@@ -130,6 +143,7 @@ __global__ void __launch_bounds__(PipeM::THREADS, MINB)
   T *FGall = reinterpret_cast<T *>(smem_raw + PM::OFF_FG);
   T *HZ = reinterpret_cast<T *>(smem_raw + PM::OFF_HZ);
   T *FF = reinterpret_cast<T *>(smem_raw + PM::OFF_FF);
+  T *QPs = reinterpret_cast<T *>(smem_raw + PM::OFF_QP);
   const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
   T *FG = FGall + w * PM::FGW;
   const int n0 = 2 * t + 8 * g + 64 * w;  // the lane's nodes n0, n0 + 1
@@ -170,6 +184,24 @@ __global__ void __launch_bounds__(PipeM::THREADS, MINB)
     }
   };
   load_nbr(0, nbn);
+  // this thread's face slots' neighbour traces of group `it` (stored values,
+  // without the offsets) into QPs, as one cp.async group
+  auto issue_qp = [&](int it, const int32_t *codes) {
+    if constexpr (!PM::ASYNC_QP) return;
+    const T *Qn = src.Qin(it);
+#pragma unroll
+    for (int u = 0; u < PM::FPT; ++u) {
+      const int fs = tid + u * PM::THREADS;
+      if (fs < PM::FSLOTS && codes[u] >= 0) {
+        const int64_t e2 = codes[u] >> 3;
+        const int vP = face_node<DIM, Nq>(codes[u] & 7, fs % Nfp);
+#pragma unroll
+        for (int s = 0; s < NS; ++s) cp_async<sizeof(T)>(QPs + s * PM::FSLOTS + fs, Qn + vP + Np * (s + NS * e2));
+      }
+    }
+    cp_async_commit();
+  };
+  if (PM::ASYNC_QP && src.valid(0)) issue_qp(0, nbn);
 
   const T *curD = nullptr;
   A Dg0 = A(0), Dg1 = A(0);  // D[t, g] and D[t + 4, g] (column-major D[m + Nq i])
@@ -199,7 +231,7 @@ __global__ void __launch_bounds__(PipeM::THREADS, MINB)
 #pragma unroll
     for (int u = 0; u < PM::FPT; ++u) nbv[u] = nbn[u];
     load_nbr(it + 1, nbn);
-    T qP[PM::FPT][NS], nrm[PM::FPT][DIM], smj[PM::FPT];
+    T qP[PM::FPT][NS], nrm[PM::FPT][DIM], smj[PM::FPT];  // qP: register traces (FP64)
 #pragma unroll
     for (int u = 0; u < PM::FPT; ++u) {
       const int fs = tid + u * PM::THREADS;
@@ -209,11 +241,13 @@ __global__ void __launch_bounds__(PipeM::THREADS, MINB)
 #pragma unroll
         for (int c = 0; c < DIM; ++c) nrm[u][c] = sgp[c];
         smj[u] = sgp[DIM];
-        if (nbv[u] >= 0) {
-          const int64_t e2 = nbv[u] >> 3;
-          const int vP = face_node<DIM, Nq>(nbv[u] & 7, fn);
+        if constexpr (!PM::ASYNC_QP) {
+          if (nbv[u] >= 0) {
+            const int64_t e2 = nbv[u] >> 3;
+            const int vP = face_node<DIM, Nq>(nbv[u] & 7, fn);
 #pragma unroll
-          for (int s = 0; s < NS; ++s) qP[u][s] = Qin[vP + Np * (s + NS * e2)] + qr[s];
+            for (int s = 0; s < NS; ++s) qP[u][s] = Qin[vP + Np * (s + NS * e2)] + qr[s];
+          }
         }
       }
     }
@@ -228,7 +262,9 @@ __global__ void __launch_bounds__(PipeM::THREADS, MINB)
     }
     if (!mbar_wait_bounded(&barS[0], (uint32_t)(it & 1), src.wait_limit())) timed_out = true;
 
-    // ---- face fluxes (any thread, any face node) into FF
+    // ---- face fluxes (any thread, any face node) into FF; FP32: the
+    // neighbour traces were copied by this thread during the previous group
+    if constexpr (PM::ASYNC_QP) cp_async_wait<0>();
 #pragma unroll
     for (int u = 0; u < PM::FPT; ++u) {
       const int fs = tid + u * PM::THREADS;
@@ -244,7 +280,12 @@ __global__ void __launch_bounds__(PipeM::THREADS, MINB)
         T PPv, riP;
         if (nbv[u] >= 0) {
 #pragma unroll
-          for (int s = 0; s < NS; ++s) qq[s] = qP[u][s];
+          for (int s = 0; s < NS; ++s) {
+            if constexpr (PM::ASYNC_QP)
+              qq[s] = QPs[s * PM::FSLOTS + fs] + qr[s];
+            else
+              qq[s] = qP[u][s];
+          }
           T gP = T(0);
           if (p.grav != T(0)) {
             const int64_t e2 = nbv[u] >> 3;
@@ -263,6 +304,8 @@ __global__ void __launch_bounds__(PipeM::THREADS, MINB)
         for (int s = 0; s < NS; ++s) FF[(f * NS + s) * Nfp + fn] = smj[u] * out[s];
       }
     }
+    // this thread has read its slots: copy the next group's traces into them
+    if (PM::ASYNC_QP && more) issue_qp(it + 1, nbn);
 
     // ---- volume fluxes of the lane's two nodes, one node at a time: F, G
     // into the warp's planes, H into the shared zeta buffer
@@ -328,6 +371,7 @@ __global__ void __launch_bounds__(PipeM::THREADS, MINB)
         atomicOr(src.status(it), ST_TIMEOUT);
         mbar_wait_bounded(&barS[0], (uint32_t)(it & 1), src.wait_limit());
       }
+      if constexpr (PM::ASYNC_QP) cp_async_wait<0>();  // this thread's trace copies land before the block leaves
       return;
     }
     if (tid == 0 && more) issue_S(it + 1);
