@@ -717,8 +717,10 @@ struct BatchSrc {
   __device__ bool last(int it) const { return at(it).last != 0; }
   __device__ int64_t e0(int it) const { return at(it).e0; }
   __device__ int nv(int it) const { return at(it).nv; }
-  __device__ const T *Qin(int it) const { return at(it).d.Q[at(it).par]; }
-  __device__ T *Qout(int it) const { return at(it).d.Q[at(it).par ^ 1]; }
+  // (par & 1: an entry that holds no item leaves par unset; the index stays
+  // inside the descriptor even if such an entry is asked)
+  __device__ const T *Qin(int it) const { return at(it).d.Q[at(it).par & 1]; }
+  __device__ T *Qout(int it) const { return at(it).d.Q[(at(it).par & 1) ^ 1]; }
   __device__ T *rhs(int it) const { return at(it).d.rhs; }
   __device__ const T *vgeo(int it) const { return at(it).d.vgeo; }
   __device__ const T *sgeo(int it) const { return at(it).d.sgeo; }

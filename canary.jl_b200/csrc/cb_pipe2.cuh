@@ -89,7 +89,13 @@ struct Pipe2 {
   static constexpr size_t FLUX = sizeof(T) * DIM * FDIR;
   static constexpr size_t OFF_FF = OFF_F + pad16(FLUX);
   static constexpr size_t FFB = P1::FFB;
-  static constexpr size_t smem() { return OFF_FF + pad16(FFB); }  // sources append their ring here
+  // FP32: the neighbour state traces of each face slot, [NS][FSLOTS], copied
+  // by the slot's thread one group ahead (cp.async) instead of loaded into
+  // registers at the top of the group
+  static constexpr bool ASYNC_QP = sizeof(T) == 4;
+  static constexpr size_t OFF_QP = OFF_FF + pad16(FFB);
+  static constexpr size_t QPB = ASYNC_QP ? sizeof(T) * NS * (size_t)C::FSLOTS : 0;
+  static constexpr size_t smem() { return OFF_QP + pad16(QPB); }  // sources append their ring here
   static constexpr size_t RING_MAX = 640;
   static constexpr bool OK = BULK && smem() + RING_MAX <= SMEM_LIMIT;
   // whether `blocks` blocks fit in one SM's shared memory (228 KB, 1 KB of
@@ -187,6 +193,7 @@ k_stage_pipe2(Src src, PhysT<T> p, T rka) {
   T *T0 = reinterpret_cast<T *>(smem_raw + PP::OFF_T);  // per slab [EPB][NS][Np] carry, then [EPB] sgeo
   T *sF = reinterpret_cast<T *>(smem_raw + PP::OFF_F);
   T *FF = reinterpret_cast<T *>(smem_raw + PP::OFF_FF);
+  T *QPs = reinterpret_cast<T *>(smem_raw + PP::OFF_QP);  // [NS][FSLOTS] (ASYNC_QP)
   const int tid = threadIdx.x;
 
   // Byte offset of a source within its 16-byte line (0 unless RAG).
@@ -281,6 +288,24 @@ k_stage_pipe2(Src src, PhysT<T> p, T rka) {
     }
   };
   load_nbr(0, nbn);
+  // this thread's face slots' neighbour traces of group `it` (stored values,
+  // without the offsets) into QPs, as one cp.async group (ASYNC_QP)
+  auto issue_qp = [&](int it, const int32_t *codes) {
+    const T *Qn = src.Qin(it);
+#pragma unroll
+    for (int u = 0; u < C::FPT; ++u) {
+      const int fs = tid + u * C::THREADS;
+      if (fs < C::FSLOTS && codes[u] >= 0) {
+        const int64_t e2 = codes[u] >> 3;
+        const int vP = face_node<DIM, Nq>(codes[u] & 7, fs % Nfp);
+#pragma unroll
+        for (int s = 0; s < NS; ++s) cp_async<sizeof(T)>(QPs + s * C::FSLOTS + fs, Qn + vP + Np * (s + NS * e2));
+      }
+    }
+    cp_async_commit();
+  };
+  if constexpr (PP::ASYNC_QP)
+    if (src.valid(0)) issue_qp(0, nbn);
   // AFF: the LGL weights head every mesh's record array (the same for every
   // mesh of this order)
   const T *WS = DT + PP::DTS;
@@ -304,20 +329,22 @@ k_stage_pipe2(Src src, PhysT<T> p, T rka) {
     for (int s = 0; s < NS; ++s) qr[s] = src.qref(it, s);
 
     // ---- neighbour traces of this group (codes were loaded one group ago)
-    T qP[C::FPT][NS];
+    T qP[C::FPT][NS];  // FP64: in registers; FP32: copied into QPs a group ago
     int32_t nbv[C::FPT];
 #pragma unroll
     for (int u = 0; u < C::FPT; ++u) nbv[u] = nbn[u];
     load_nbr(it + 1, nbn);
+    if constexpr (!PP::ASYNC_QP) {
 #pragma unroll
-    for (int u = 0; u < C::FPT; ++u) {
-      const int fs = tid + u * C::THREADS;
-      const int fn = fs % Nfp;
-      if (nbv[u] >= 0) {
-        const int64_t e2 = nbv[u] >> 3;
-        const int vP = face_node<DIM, Nq>(nbv[u] & 7, fn);
+      for (int u = 0; u < C::FPT; ++u) {
+        const int fs = tid + u * C::THREADS;
+        const int fn = fs % Nfp;
+        if (nbv[u] >= 0) {
+          const int64_t e2 = nbv[u] >> 3;
+          const int vP = face_node<DIM, Nq>(nbv[u] & 7, fn);
 #pragma unroll
-        for (int s = 0; s < NS; ++s) qP[u][s] = Qin[vP + Np * (s + NS * e2)] + qr[s];
+          for (int s = 0; s < NS; ++s) qP[u][s] = Qin[vP + Np * (s + NS * e2)] + qr[s];
+        }
       }
     }
 
@@ -393,6 +420,7 @@ k_stage_pipe2(Src src, PhysT<T> p, T rka) {
         buoy[u] = MJ * q[IR] * p.grav;
       }
     }
+    if constexpr (PP::ASYNC_QP) cp_async_wait<0>();  // this thread's traces, copied a group ago
 #pragma unroll
     for (int u = 0; u < C::FPT; ++u) {
       const int fs = tid + u * C::THREADS;
@@ -421,7 +449,12 @@ k_stage_pipe2(Src src, PhysT<T> p, T rka) {
         T PPv, riP;
         if (nbv[u] >= 0) {
 #pragma unroll
-          for (int s = 0; s < NS; ++s) qq[s] = qP[u][s];
+          for (int s = 0; s < NS; ++s) {
+            if constexpr (PP::ASYNC_QP)
+              qq[s] = QPs[s * C::FSLOTS + fs] + qr[s];
+            else
+              qq[s] = qP[u][s];
+          }
           T gP = T(0);
           if (!AFF && p.grav != T(0)) {
             const int64_t e2 = nbv[u] >> 3;
@@ -440,6 +473,10 @@ k_stage_pipe2(Src src, PhysT<T> p, T rka) {
         for (int s = 0; s < NS; ++s) FF[(f * NS + s) * FS + el * Nfp + fn] = smj * out[s];
       }
     }
+    // this thread has read its slots: copy the next group's traces into them
+    // (only for a valid group: an empty ring entry holds no instance)
+    if constexpr (PP::ASYNC_QP)
+      if (src.valid(it + 1)) issue_qp(it + 1, nbn);
     // The mid-iteration barrier also agrees on whether any thread's wait gave
     // up.  If one did, the block stores nothing for this group (its slabs may
     // be incomplete), flags the status word, lets the copies it has issued
@@ -456,6 +493,7 @@ k_stage_pipe2(Src src, PhysT<T> p, T rka) {
         for (int g = it; g <= it + PP::LOOK && src.valid(g); ++g)
           mbar_wait_bounded(&barT[g % PP::NTB], (uint32_t)((g / PP::NTB) & 1), src.wait_limit());
       }
+      if constexpr (PP::ASYNC_QP) cp_async_wait<0>();  // this thread's trace copies land before it leaves
       return;
     }
     // S[sb] is no longer read: refill it while phase B runs
