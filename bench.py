@@ -588,17 +588,21 @@ def main():
     # the state from pinned host memory, advances one step and reads the
     # state back (the step's input is the state alone: the 2N-storage carry
     # is zero at a step boundary, scaled by RKA[0] = 0 after the fifth stage).
-    # Two device states, each with its own solver on the compute stream, and
+    # Three device states, each with its own solver on the compute stream, and
     # one copy stream per direction: the upload of step k+1 and the read-back
-    # of step k overlap step k's compute and each other.
+    # of step k overlap step k's compute and each other, and the upload of
+    # step k+3 waits only for the read-back of step k (with two states the
+    # cycle upload -> step -> read-back of every second step serialises).
+    NB = 3
     hQ = torch.empty(dQ.numel(), dtype=real, pin_memory=True)
     hQ.copy_(dQ)
-    hout = [torch.empty_like(hQ, pin_memory=True) for _ in range(2)]
-    dQ2 = [dQ, torch.empty_like(dQ)]
-    rhs2 = [drhs, torch.zeros_like(drhs)]
-    solvers = [solver, dg.LSRK(dm, dQ2[1], rhs2[1], args.precision, dg.make_phys(), stream)]
-    solvers[1].set_offset(off)
-    solvers[1].set_kernel(args.stage_kernel)
+    hout = [torch.empty_like(hQ, pin_memory=True) for _ in range(NB)]
+    dQ2 = [dQ] + [torch.empty_like(dQ) for _ in range(NB - 1)]
+    rhs2 = [drhs] + [torch.zeros_like(drhs) for _ in range(NB - 1)]
+    solvers = [solver] + [dg.LSRK(dm, dQ2[i], rhs2[i], args.precision, dg.make_phys(), stream) for i in range(1, NB)]
+    for sv in solvers[1:]:
+        sv.set_offset(off)
+        sv.set_kernel(args.stage_kernel)
     up, down = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
     torch.cuda.synchronize(dev)
     if tdist is not None:
@@ -608,9 +612,9 @@ def main():
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     f0.record(up)
     for k in range(args.e2e_steps):
-        b = k % 2
-        if k >= 2:
-            up.wait_event(stored[k - 2])  # state buffer b has been read back
+        b = k % NB
+        if k >= NB:
+            up.wait_event(stored[k - NB])  # state buffer b has been read back
         with torch.cuda.stream(up):
             dQ2[b].copy_(hQ, non_blocking=True)
         loaded.append(ev())
@@ -627,7 +631,7 @@ def main():
     f1.record(down)
     torch.cuda.synchronize(dev)
     e2e_ms = replicas.max_over_ranks(f0.elapsed_time(f1), device=dev)
-    e2e_ok = bool(torch.equal(hout[(args.e2e_steps - 1) % 2], hout[(args.e2e_steps - 2) % 2]))
+    e2e_ok = bool(torch.equal(hout[(args.e2e_steps - 1) % NB], hout[(args.e2e_steps - 2) % NB]))
     for sv in solvers:
         sv.close()
     del dQ2, rhs2, hout
@@ -671,7 +675,7 @@ def main():
         "e2e": {"value": world * dof * 5 * args.e2e_steps / (e2e_ms * 1e-3), "unit": METRIC,
                 "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo, "steps": args.e2e_steps,
                 "ms_per_step": e2e_ms / args.e2e_steps, "results_repeat": e2e_ok,
-                "how": "cb_solver per state buffer; H2D, step and D2H on three streams, two states in flight"},
+                "how": "cb_solver per state buffer; H2D, step and D2H on three streams, three states in flight"},
         "gpu_launches": launches,
         "clocks": clk,
     }
