@@ -51,26 +51,22 @@ struct alignas(16) BWork {
   int32_t slot, e0, nv, valid;
 };
 
-// Stage variants of one (dim, N): 0 = the pipelined bulk-copy stage
-// (k_stage_pipe2, groups of Cfg::EPB elements, state/metric/carry/face
-// geometry staged one group ahead) at its default occupancy (Pipe2::MINB
-// resident blocks per SM), 1 and 2 = the grouped stage with groups of about
-// 256 and 512 nodes, 3 and 4 = the pipelined stage compiled for the two other
-// occupancies among 2, 3 and 4 blocks per SM (blocks of up to 256 threads).
-// Shape id of (dim, N, variant); ids of shapes that are not built stay
-// unused.
-// Stage variants per (dim, N): 0 pipelined (default occupancy), 1 / 2
+// Stage variants per (dim, N): 0 pipelined (k_stage_pipe2, groups of
+// Cfg::EPB elements staged one group ahead, default occupancy), 1 / 2
 // grouped (~256 / ~512 nodes), 3 / 4 pipelined at other occupancies,
 // VAR_DEEP pipelined with copies two groups ahead, VAR_WIDE pipelined with
 // twice the elements per group on 512-thread blocks, VAR_NPT2 pipelined with
 // two nodes per thread (half the threads), and the affine-element stages
 // (affine-element geometry, copies two groups ahead) VAR_AFFINE and
 // VAR_AFFINE_NPT2 (two nodes per thread).  Affine variants run only on
-// meshes whose elements are all affine (gravity off); by default the batch
-// uses VAR_AFFINE in place of a pipelined variant for such meshes.  VAR_MMA
+// meshes whose elements are all affine (gravity off); when no variant was
+// chosen for a shape the batch uses VAR_AFFINE in place of its default
+// pipelined variant for such meshes.  VAR_MMA
 // is the tensor-core stage (k_stage_mma, 3-D N = 7).
 constexpr int VAR_AFFINE = 5, VAR_DEEP = 6, VAR_WIDE = 7, VAR_NPT2 = 8, VAR_AFFINE_NPT2 = 9, VAR_MMA = 10, NVAR = 11;
 __host__ __device__ constexpr bool var_affine(int var) { return var == VAR_AFFINE || var == VAR_AFFINE_NPT2; }
+// Shape id of (dim, N, variant); ids of shapes that are not built stay
+// unused.
 constexpr int NSHAPE = 2 * NVAR * (BMAXN2 + 1);
 __host__ __device__ constexpr int shape_id(int dim, int N, int var) {
   return (dim - 2) * NVAR * (BMAXN2 + 1) + NVAR * N + var;
