@@ -23,6 +23,7 @@ After the timed region (one GPU) the line also carries:
   * parity.timed_workload: the timed workload advanced by 200 steps on the GPU and
     by the oracle from the same device-built mesh and state (bar 1e-12); the
     oracle's timing on all host cores is the cpu_baseline;
+  * fp32_form: the timed workload in the FP32 form, timed the same way;
   * precision_form: FP32 against FP64 at 32^3, N = 4, 7, 10, 1000 steps, the
     LDG Navier-Stokes variant and the 2-D vortex (bar 1e-5);
   * batched: 512 vortex instances in one batch per precision, with a roofline
@@ -429,6 +430,39 @@ def batched_ensemble(count=512, seed=0, steps=500, device="cuda", parity_sample=
     return out
 
 
+def fp32_form(args, dev, stream):
+    """The timed workload in the FP32 form (state stored as its deviation
+    from the per-field mean, FP32 arithmetic), args.warmup + args.steps steps
+    with CUDA events around args.steps of them; throughput and roofline."""
+    import torch
+    from canary_b200 import dg
+    dm, dQ, drhs, dt, off = setup_device_workload(args.n_side, args.order, 32, device=dev)
+    s = dg.LSRK(dm, dQ, drhs, 32, dg.make_phys(), stream)
+    s.set_offset(off)
+    s.run(args.warmup, dt)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    s.run(args.steps, dt)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1)
+    kernel = "k_stage_mma" if s.kernel == 2 else "k_stage_pipe2"
+    finite = bool(np.all(np.isfinite(s.sums())))
+    s.close()
+    mesh = dm.mesh
+    dof = mesh.nelem * mesh.Np * 5
+    t_launch = ms * 1e-3 / (5 * args.steps)
+    bpn = bytes_per_node(3, args.order, 4)
+    peak, peak_kind = measured_peaks()
+    achieved = mesh.nelem * mesh.Np * bpn / t_launch / 1e9
+    return {"value": dof * 5 * args.steps / (ms * 1e-3), "unit": METRIC, "ms_per_step": ms / args.steps,
+            "steps": args.steps, "dtype": "f32", "state_finite": finite,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": peak_kind, "bytes_per_node": bpn, "kernel": kernel,
+                         "launch_ms": t_launch * 1e3}}
+
+
 def dist_init():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     if ws <= 1:
@@ -529,6 +563,8 @@ def main():
     ap.add_argument("--batched-precisions", type=int, nargs="+", default=[64, 32], choices=[64, 32])
     ap.add_argument("--no-autotune", action="store_true",
                     help="batched section: the batch's default stage variants instead of the autotuner's")
+    ap.add_argument("--no-fp32-form", action="store_true",
+                    help="skip the FP32 form of the timed workload (run on 1 GPU, FP64 arm only)")
     ap.add_argument("--no-served", action="store_true",
                     help="skip the served-stream measurement (run on 1 GPU only)")
     ap.add_argument("--served-requests", type=int, default=150)
@@ -641,6 +677,11 @@ def main():
     par = None
     if rank == 0 and world == 1 and args.precision == 64 and args.parity_steps > 0:
         par = Config1Parity(dm, dQ0, dt, args.parity_steps, stream, os.cpu_count() or 1)
+    # the FP32 form of the same workload (offsets, FP32 state and arithmetic,
+    # FP64-computed geometry rounded once), timed like the FP64 line
+    fp32 = None
+    if world == 1 and args.precision == 64 and not args.no_fp32_form:
+        fp32 = fp32_form(args, dev, stream)
     prec_sec = None
     if world == 1 and args.precision_steps > 0:
         prec_sec = precision_section(args.precision_steps, device=dev)
@@ -679,6 +720,9 @@ def main():
         "gpu_launches": launches,
         "clocks": clk,
     }
+    if fp32 is not None:
+        fp32["over_fp64_plain"] = fp32["value"] / value
+        line["fp32_form"] = fp32
     if prec_sec is not None:
         line["precision_form"] = prec_sec
     if par is not None:
