@@ -14,8 +14,10 @@
 //   * the metric, residual carry and face geometry are each read by the one
 //     thread that needs them, from L2, where a block-wide L2 prefetch issued
 //     at the top of the group's iteration has placed them;
-//   * neighbour traces (state and gradient) are read in the face phase,
-//     their neighbour codes one group ahead.
+//   * neighbour codes are loaded one group ahead; the neighbour traces
+//     (state and gradient) are read in the face phase (FP64) or copied into
+//     shared memory one group ahead by the face slot's thread (cp.async;
+//     FP32).
 //
 // Groups, flux rows and the face buffer are those of k_stage_pipe2
 // (Cfg<DIM, Nq>), so a batch's work list is the same for the grouped
@@ -46,7 +48,14 @@ struct NsPipe {
   static constexpr size_t OFF_F = OFF_G + GS;
   static constexpr size_t FDIR = P1::FDIR;
   static constexpr size_t OFF_FF = OFF_F + pad16(sizeof(T) * DIM * FDIR);
-  static constexpr size_t smem() { return OFF_FF + pad16(P1::FFB); }  // sources append their ring here
+  // FP32: the neighbour traces of each face slot — state [NS] and gradient
+  // [NS*DIM] — copied by the slot's thread one group ahead (cp.async),
+  // [NS*(DIM+1)][FSLOTS]
+  static constexpr bool ASYNC_TR = sizeof(T) == 4;
+  static constexpr int TRV = NS * (DIM + 1);
+  static constexpr size_t OFF_TR = OFF_FF + pad16(P1::FFB);
+  static constexpr size_t TRB = ASYNC_TR ? sizeof(T) * TRV * (size_t)C::FSLOTS : 0;
+  static constexpr size_t smem() { return OFF_TR + pad16(TRB); }  // sources append their ring here
   static constexpr size_t RING_MAX = 640;
   static constexpr int MINB = C::THREADS <= 256 ? 2 : 1;
   static constexpr bool OK = MINB * (smem() + RING_MAX + 1024) <= 228 * 1024 && smem() + RING_MAX <= SMEM_LIMIT;
@@ -78,6 +87,7 @@ k_ns_stage_pipe(Src src, PhysT<T> p, T rka) {
   T *Sg0 = reinterpret_cast<T *>(smem_raw + PP::OFF_G);  // [EPB][DIM][NS][Np] gradient
   T *sF = reinterpret_cast<T *>(smem_raw + PP::OFF_F);
   T *FF = reinterpret_cast<T *>(smem_raw + PP::OFF_FF);
+  T *TR = reinterpret_cast<T *>(smem_raw + PP::OFF_TR);  // [TRV][FSLOTS] (ASYNC_TR)
   const int tid = threadIdx.x;
 
   auto head_of = [](const T *g) -> uint32_t {
@@ -141,6 +151,27 @@ k_ns_stage_pipe(Src src, PhysT<T> p, T rka) {
     }
   };
   load_nbr(0, nbn);
+  // this thread's face slots' neighbour traces of group `it` (state as
+  // stored, without offsets, and gradient) into TR, one cp.async group
+  auto issue_tr = [&](int it, const int32_t *codes) {
+    const T *Qn = src.Qin(it), *Gn = src.gq(it);
+#pragma unroll
+    for (int u = 0; u < C::FPT; ++u) {
+      const int fs = tid + u * C::THREADS;
+      if (fs < C::FSLOTS && codes[u] >= 0) {
+        const int64_t e2 = codes[u] >> 3;
+        const int vP = face_node<DIM, Nq>(codes[u] & 7, fs % Nfp);
+#pragma unroll
+        for (int s = 0; s < NS; ++s) cp_async<sizeof(T)>(TR + s * C::FSLOTS + fs, Qn + vP + Np * (s + NS * e2));
+#pragma unroll
+        for (int v = 0; v < NS * DIM; ++v)  // v = s + NS * c
+          cp_async<sizeof(T)>(TR + (NS + v) * C::FSLOTS + fs, Gn + vP + Np * (v + (int64_t)NS * DIM * e2));
+      }
+    }
+    cp_async_commit();
+  };
+  if constexpr (PP::ASYNC_TR)
+    if (src.valid(0)) issue_tr(0, nbn);
 
   bool timed_out = false;
   const T *curD = nullptr;
@@ -240,6 +271,8 @@ k_ns_stage_pipe(Src src, PhysT<T> p, T rka) {
     }
 
     // ---- face terms sMJ (Rusanov - μ n·(F_visc⁻ + F_visc⁺)/2) into FF
+    // (FP32: the neighbour traces were copied by this thread a group ago)
+    if constexpr (PP::ASYNC_TR) cp_async_wait<0>();
 #pragma unroll
     for (int u = 0; u < C::FPT; ++u) {
       const int fs = tid + u * C::THREADS;
@@ -265,7 +298,12 @@ k_ns_stage_pipe(Src src, PhysT<T> p, T rka) {
         T PPv, riP;
         if (nb >= 0) {
 #pragma unroll
-          for (int s = 0; s < NS; ++s) qq[s] = Qin[vP + Np * (s + NS * e2)] + qr[s];
+          for (int s = 0; s < NS; ++s) {
+            if constexpr (PP::ASYNC_TR)
+              qq[s] = TR[s * C::FSLOTS + fs] + qr[s];
+            else
+              qq[s] = Qin[vP + Np * (s + NS * e2)] + qr[s];
+          }
           const T gP = p.grav != T(0) ? vgeo[vP + Np * (GC + NVG * e2)] : T(0);
           riP = T(1) / qq[IR];
           PPv = pressure_ri<DIM, T>(qq, riP, gP, p);
@@ -300,7 +338,12 @@ k_ns_stage_pipe(Src src, PhysT<T> p, T rka) {
 #pragma unroll
             for (int s = 0; s < NS; ++s)
 #pragma unroll
-              for (int c = 0; c < DIM; ++c) g[s][c] = gq[vP + Np * (s + NS * (c + (int64_t)DIM * e2))];
+              for (int c = 0; c < DIM; ++c) {
+                if constexpr (PP::ASYNC_TR)
+                  g[s][c] = TR[(NS + s + NS * c) * C::FSLOTS + fs];
+                else
+                  g[s][c] = gq[vP + Np * (s + NS * (c + (int64_t)DIM * e2))];
+              }
           } else {  // mirrored gradients, the temperature gradient copied from the interior
 #pragma unroll
             for (int s = 0; s < NS; ++s) {
@@ -324,6 +367,9 @@ k_ns_stage_pipe(Src src, PhysT<T> p, T rka) {
           FF[(f * NS + s) * FS + el * Nfp + fn] = smj * out[s] - p.visc * (smj * (T(0.5) * av[s]));
       }
     }
+    // this thread has read its slots: copy the next group's traces into them
+    if constexpr (PP::ASYNC_TR)
+      if (more) issue_tr(it + 1, nbn);
     // Mid-group barrier; agrees on whether a wait gave up (then: store
     // nothing, flag the status, let the issued copy land, leave).
     if (__syncthreads_or(timed_out)) {
@@ -331,6 +377,7 @@ k_ns_stage_pipe(Src src, PhysT<T> p, T rka) {
         atomicOr(src.status(it), ST_TIMEOUT);
         mbar_wait_bounded(bar, (uint32_t)(it & 1), src.wait_limit());
       }
+      if constexpr (PP::ASYNC_TR) cp_async_wait<0>();  // this thread's trace copies land before it leaves
       return;
     }
     // the slabs are no longer read: refill them while the update runs
