@@ -432,7 +432,12 @@ struct NsGradPipe {
   static constexpr size_t OFF_F = OFF_S + PS::QS;
   static constexpr size_t OFF_FF = OFF_F + pad16(sizeof(T) * DIM * P1::FDIR);
   static constexpr size_t FFB = sizeof(T) * (size_t)C::NFACE * ND * C::EPB * C::Nfp;
-  static constexpr size_t smem() { return OFF_FF + pad16(FFB); }  // sources append their ring here
+  // FP32: the neighbour state traces of each face slot, [NS][FSLOTS], copied
+  // by the slot's thread one group ahead (cp.async)
+  static constexpr bool ASYNC_TR = sizeof(T) == 4;
+  static constexpr size_t OFF_TR = OFF_FF + pad16(FFB);
+  static constexpr size_t TRB = ASYNC_TR ? sizeof(T) * NS * (size_t)C::FSLOTS : 0;
+  static constexpr size_t smem() { return OFF_TR + pad16(TRB); }  // sources append their ring here
   static constexpr int MINB = PS::MINB;
   static constexpr bool OK = MINB * (smem() + PS::RING_MAX + 1024) <= 228 * 1024 && smem() + PS::RING_MAX <= SMEM_LIMIT;
 };
@@ -455,6 +460,7 @@ k_ns_grad_pipe(Src src, PhysT<T> p, T) {
   T *Sq0 = reinterpret_cast<T *>(smem_raw + PP::OFF_S);  // [EPB][NS][Np] state
   T *sF = reinterpret_cast<T *>(smem_raw + PP::OFF_F);   // flux rows of one gradient component
   T *FF = reinterpret_cast<T *>(smem_raw + PP::OFF_FF);  // [NF][NS*DIM][FS] face terms
+  T *TR = reinterpret_cast<T *>(smem_raw + PP::OFF_TR);  // [NS][FSLOTS] (ASYNC_TR)
   const int tid = threadIdx.x;
 
   auto head_of = [](const T *g) -> uint32_t {
@@ -503,6 +509,24 @@ k_ns_grad_pipe(Src src, PhysT<T> p, T) {
     }
   };
   load_nbr(0, nbn);
+  // this thread's face slots' neighbour state traces of group `it` (as
+  // stored) into TR, one cp.async group (ASYNC_TR)
+  auto issue_tr = [&](int it, const int32_t *codes) {
+    const T *Qn = src.Qin(it);
+#pragma unroll
+    for (int u = 0; u < C::FPT; ++u) {
+      const int fs = tid + u * C::THREADS;
+      if (fs < C::FSLOTS && codes[u] >= 0) {
+        const int64_t e2 = codes[u] >> 3;
+        const int vP = face_node<DIM, Nq>(codes[u] & 7, fs % Nfp);
+#pragma unroll
+        for (int s = 0; s < NS; ++s) cp_async<sizeof(T)>(TR + s * C::FSLOTS + fs, Qn + vP + Np * (s + NS * e2));
+      }
+    }
+    cp_async_commit();
+  };
+  if constexpr (PP::ASYNC_TR)
+    if (src.valid(0)) issue_tr(0, nbn);
 
   bool timed_out = false;
   const T *curD = nullptr;
@@ -558,6 +582,8 @@ k_ns_grad_pipe(Src src, PhysT<T> p, T) {
       }
     }
     // ---- face averages of the primitives (flux_grad!) for every component
+    // (FP32: the neighbour traces were copied by this thread a group ago)
+    if constexpr (PP::ASYNC_TR) cp_async_wait<0>();
 #pragma unroll
     for (int u = 0; u < C::FPT; ++u) {
       const int fs = tid + u * C::THREADS;
@@ -580,7 +606,12 @@ k_ns_grad_pipe(Src src, PhysT<T> p, T) {
           const int vP = face_node<DIM, Nq>(nb & 7, fn);
           T qP[NS];
 #pragma unroll
-          for (int s = 0; s < NS; ++s) qP[s] = Qin[vP + Np * (s + NS * e2)] + qr[s];
+          for (int s = 0; s < NS; ++s) {
+            if constexpr (PP::ASYNC_TR)
+              qP[s] = TR[s * C::FSLOTS + fs] + qr[s];
+            else
+              qP[s] = Qin[vP + Np * (s + NS * e2)] + qr[s];
+          }
           const T gP = p.grav != T(0) ? vgeo[vP + Np * (GC + NVG * e2)] : T(0);
           primitives<DIM, T>(qP, gP, p, pP);
         } else {  // reflective wall: mirrored velocity, same density and temperature
@@ -599,6 +630,9 @@ k_ns_grad_pipe(Src src, PhysT<T> p, T) {
         }
       }
     }
+    // this thread has read its slots: copy the next group's traces into them
+    if constexpr (PP::ASYNC_TR)
+      if (more) issue_tr(it + 1, nbn);
     // ---- per gradient component: flux rows, contraction (subtracted), face
     // terms in face order, ×MJI into gQ (unrolled: the metric column is
     // chosen at compile time, not by indexing a register array)
@@ -628,6 +662,7 @@ k_ns_grad_pipe(Src src, PhysT<T> p, T) {
             atomicOr(src.status(it), ST_TIMEOUT);
             mbar_wait_bounded(bar, (uint32_t)(it & 1), src.wait_limit());
           }
+          if constexpr (PP::ASYNC_TR) cp_async_wait<0>();  // this thread's trace copies land before it leaves
           return;
         }
         if (tid == 0 && more) issue(it + 1);
