@@ -112,6 +112,30 @@ def test_fp32_tensor_core_stage(n, nsteps, walls):
     assert _relerr(out[2], out[1]) < 1e-6
 
 
+@pytest.mark.parametrize("precision,tol", [(64, 1e-12), (32, 1e-5)])
+def test_every_kernel_choice_matches_the_oracle(precision, tol):
+    """Kernel choices 0 (default: tensor-core stage), 1 (pipelined CUDA-core
+    stage), 2 (tensor-core) and 3 (unpipelined grouped stage) on one warped
+    3-D N=7 mesh: each against the oracle at the form's bar (FP64 1e-12, FP32
+    1e-5), and the FP64 ones with each other to round-off (1e-13)."""
+    m, Q, dt = _case(3, seed=5, walls=True)
+    ref, rref = Q.copy(order="F"), np.zeros_like(Q, order="F")
+    O.lowstorageRK(3, 7, m.vgeo, m.sgeo, ref, rref, m.D, dt, 3, m.vmapM, m.vmapP, m.elemtobndy, _phys(), NT)
+    dm = dg.DeviceMesh.upload(m)
+    out = {}
+    for kernel in (0, 1, 2, 3):
+        s = dg.LSRK.for_state(dm, Q, precision)
+        s.set_kernel(kernel)
+        assert s.kernel == (2 if kernel == 0 else kernel)
+        s.run(3, dt)
+        out[kernel] = s.state()
+        s.close()
+        assert _relerr(out[kernel], ref) < tol, kernel
+    if precision == 64:
+        for kernel in (1, 2, 3):
+            assert _relerr(out[kernel], out[0]) < 1e-13
+
+
 def test_kernel_choice_is_checked():
     m, Q, dt = _case(2)
     dm = dg.DeviceMesh.upload(m)
