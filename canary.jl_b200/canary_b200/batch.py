@@ -27,9 +27,10 @@ MAX_ORDER = {2: 8, 3: 7}  # orders compiled into the batched stage
 # group on 512-thread blocks, 8 = pipelined staging with two nodes per thread;
 # 5 / 9 = the affine-element stage (copies two groups ahead) with one / two
 # nodes per thread, for meshes whose elements are all affine; 10 = the
-# tensor-core stage (3-D N = 7)
-VARIANTS = (0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10)
-PIPELINED = (0, 3, 4, 6, 7, 8)  # per-node geometry, bit-identical among themselves
+# tensor-core stage (3-D N = 7); 11 = the lean pipelined stage (only the state
+# staged in shared memory, geometry and carry read from L2)
+VARIANTS = (0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11)
+PIPELINED = (0, 3, 4, 6, 7, 8, 11)  # per-node geometry, bit-identical among themselves
 AFFINE = (5, 9)  # affine-element geometry, bit-identical among themselves
 VAR_AFFINE = 5
 VAR_DEEP = 6
@@ -37,6 +38,7 @@ VAR_WIDE = 7
 VAR_NPT2 = 8
 VAR_AFFINE_NPT2 = 9
 VAR_MMA = 10
+VAR_LEAN = 11
 
 
 class BatchMesh:
@@ -455,10 +457,16 @@ def autotune(precision: int, shapes, nodes_target: int = 8_000_000, steps: int =
                 b.run(steps)
                 ev1.record()
                 torch.cuda.synchronize()
-                ts.append(ev0.elapsed_time(ev1))
+                ts.append(ev0.elapsed_time(ev1) / steps)
             timings[var] = min(ts)
             b.release(slot)
             b.close()
         bm.close()
         best[(dim, N)] = min(timings, key=timings.get)
+        if report is not None:
+            info = Batch(precision, 1)
+            report[(dim, N)] = {"variant": best[(dim, N)], "instances": 1, "admitted": 1,
+                                "nodes": bm.Np * bm.nelem, "ms_per_step": timings,
+                                "config": info.variant_info(dim, N, best[(dim, N)])}
+            info.close()
     return best

@@ -440,13 +440,14 @@ class LSRK:
         """Stage kernel: 0 = the shape's default, 1 = the CUDA-core stages,
         2 = the tensor-core (DMMA) stage of the inviscid 3-D N=7 form, 3 = the
         unpipelined grouped stages (for the fused viscous form: the grouped
-        stage pass instead of the pipelined one)."""
+        passes instead of the pipelined ones), 4 = the lean pipelined stage
+        of the inviscid form (only the state staged in shared memory)."""
         check(_lib.lib().cb_solver_set_kernel(self._h, int(kernel)))
 
     @property
     def kernel(self) -> int:
         """The stage kernel the solver runs: 1 CUDA-core, 2 tensor-core, 3
-        grouped."""
+        grouped, 4 lean."""
         v = C.c_int(0)
         check(_lib.lib().cb_solver_get_kernel(self._h, C.byref(v)))
         return v.value

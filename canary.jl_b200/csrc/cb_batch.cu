@@ -198,7 +198,19 @@ constexpr int VAR_VISC = 1;
 // (the autotuner may choose another)
 template <typename T>
 int b_default_var(int dim, int N) {
-  if (dim == 3 && N == 7 && PipeMT<T>::DEFAULT && b_var_ok<T>(dim, N, VAR_MMA)) return VAR_MMA;
+  // 3-D defaults from the autotuner's B200 timings of one 6 M-node warped
+  // instance (ms per step): FP64 N=3 lean 3.03 against 4.11 for variant 0,
+  // N=4 3.46 against 4.46; FP32 N=4 variant 4 1.57 against 1.86, N=5
+  // variant 3 1.34 against 1.39, N=6 variant 8 1.48 against 1.77; N=7 the
+  // tensor-core stage (2.15 / 1.12 against 2.26 / 1.42)
+  auto pick = [&](int v) { return b_var_ok<T>(dim, N, v) ? v : -1; };
+  int v = -1;
+  if (dim == 3 && N == 7 && PipeMT<T>::DEFAULT) v = pick(VAR_MMA);
+  else if (dim == 3 && sizeof(T) == 8 && (N == 3 || N == 4)) v = pick(VAR_LEAN);
+  else if (dim == 3 && sizeof(T) == 4 && N == 4) v = pick(4);
+  else if (dim == 3 && sizeof(T) == 4 && N == 5) v = pick(3);
+  else if (dim == 3 && sizeof(T) == 4 && N == 6) v = pick(VAR_NPT2);
+  if (v >= 0) return v;
   return b_var_ok<T>(dim, N, 0) ? 0 : b_var_ok<T>(dim, N, 2) ? 2 : 1;
 }
 // Shared-memory limit and persistent grid (all SMs at the occupancy that the

@@ -62,8 +62,10 @@ struct alignas(16) BWork {
 // meshes whose elements are all affine (gravity off); when no variant was
 // chosen for a shape the batch uses VAR_AFFINE in place of its default
 // pipelined variant for such meshes.  VAR_MMA
-// is the tensor-core stage (k_stage_mma, 3-D N = 7).
-constexpr int VAR_AFFINE = 5, VAR_DEEP = 6, VAR_WIDE = 7, VAR_NPT2 = 8, VAR_AFFINE_NPT2 = 9, VAR_MMA = 10, NVAR = 11;
+// is the tensor-core stage (k_stage_mma, 3-D N = 7), VAR_LEAN the lean
+// pipelined stage (k_stage_lean: only the state staged in shared memory).
+constexpr int VAR_AFFINE = 5, VAR_DEEP = 6, VAR_WIDE = 7, VAR_NPT2 = 8, VAR_AFFINE_NPT2 = 9, VAR_MMA = 10,
+              VAR_LEAN = 11, NVAR = 12;
 __host__ __device__ constexpr bool var_affine(int var) { return var == VAR_AFFINE || var == VAR_AFFINE_NPT2; }
 // Shape id of (dim, N, variant); ids of shapes that are not built stay
 // unused.
@@ -790,6 +792,17 @@ void b_fill(BKernels<T> &k) {
     using PD = Pipe2<DIM, Nq, T, true, true>;
     if constexpr (PD::OK && PD::fits(M0)) b_fill_pipe<DIM, Nq, T, M0, true, true>(k, VAR_AFFINE);
     else if constexpr (Pipe2<DIM, Nq, T, true>::OK) b_fill_pipe<DIM, Nq, T, M0, true>(k, VAR_AFFINE);
+    // the lean pipelined stage (state-only staging)
+    if constexpr (Lean<DIM, Nq, T>::OK) {
+      using Src = BatchSrc<T, Lay<DIM>::NS, Cfg<DIM, Nq>::EPB, 3>;
+      const int id = shape_id(DIM, N, VAR_LEAN);
+      k.fn[id] = (const void *)k_stage_lean<DIM, Nq, T, Src>;
+      k.epb[id] = Cfg<DIM, Nq>::EPB;
+      k.threads[id] = Cfg<DIM, Nq>::THREADS;
+      k.smem[id] = Lean<DIM, Nq, T>::smem() + Src::RING_BYTES;
+      k.pipelined[id] = true;
+      k.ahead[id] = 1;
+    }
     // the tensor-core stage (3-D N = 7, one element per group)
     if constexpr (DIM == 3 && Nq == 8) {
       using PM = PipeMT<T>;

@@ -760,6 +760,7 @@ __global__ void k_round_f32(float *__restrict__ dst, const double *__restrict__ 
 #include "cb_pipe2.cuh"
 #include "cb_mma.cuh"
 #include "cb_ns_pipe.cuh"
+#include "cb_lean.cuh"
 namespace cb {
 
 // ---------------------------------------------------------------- launchers
@@ -802,6 +803,23 @@ struct Launch {
   // Whether kernel 0 (the shape's default) is the tensor-core stage: the
   // faster of the two on B200 at the benchmark size.
   static constexpr bool MMA_DEFAULT = MMA_OK && PipeMT<T>::DEFAULT;
+  // Whether the lean pipelined stage is built for this shape, and whether it
+  // is the shape's default (where the tensor-core stage is not).
+  static constexpr bool LEAN_OK = Lean<DIM, Nq, T>::OK;
+  // Default stage kernel per shape, from B200 timings of one mesh (ms per
+  // step, warped 3-D cubes of 7-17 M nodes; pipelined CUDA-core / grouped /
+  // lean): FP64 N=3 3.66 / 3.34 / 2.76, N=4 4.95 / 4.20 / 3.78, N=5 2.37 /
+  // 3.45 / 2.67, N=6 3.37 / 5.13 / 3.83, N=8 5.78 / 5.71 / 5.33; FP32 N=3
+  // 1.34 / 1.31 / 1.66, N=4 2.61 / 1.75 / 2.26, N=5 1.65 / 1.44 / 1.72, N=6
+  // 2.02 / 1.68 / 2.61, N=8 3.08 / 2.61 / 3.44, N=9 2.22 / 1.93 / 2.45 (the
+  // FP32 pipelined plans fit fewer blocks per SM than the grouped stage).
+  // 3-D N=7 runs the tensor-core stage in both precisions.
+  static constexpr int DEFAULT_KERNEL =
+      MMA_DEFAULT ? 2
+      : DIM == 3 && sizeof(T) == 8 && LEAN_OK && (Nq == 4 || Nq == 5 || Nq == 9) ? 4
+      : DIM == 3 && sizeof(T) == 4 && Nq >= 4 && Nq <= 10 ? 3
+      : 1;
+  static constexpr bool LEAN_DEFAULT = DEFAULT_KERNEL == 4;
   // Resident blocks per SM of a kernel at `smem` bytes, from the occupancy
   // calculator, cached per device in `cache`.
   template <typename K>
@@ -824,7 +842,8 @@ struct Launch {
   // kernel: 0 = the default for the shape (the tensor-core stage where it is
   // built, else the pipelined CUDA-core stage, else the older ones), 1 = the
   // CUDA-core stages only, 2 = the tensor-core stage (cudaErrorNotSupported
-  // where it is not built), 3 = the unpipelined grouped stage k_stage.  probe != 0: the timeout test hook of the
+  // where it is not built), 3 = the unpipelined grouped stage k_stage, 4 =
+  // the lean pipelined stage k_stage_lean (state-only staging).  probe != 0: the timeout test hook of the
   // pipelined stages (see MeshSrc); shapes without one return
   // cudaErrorNotSupported for it.
   // ebeg: the launch covers elements ebeg .. nelem - 1 (neighbour indices
@@ -838,6 +857,10 @@ struct Launch {
     const bool aligned = ((reinterpret_cast<uintptr_t>(Qin) | reinterpret_cast<uintptr_t>(vgeo)) & 15) == 0;
     const bool aligned2 = aligned && ((reinterpret_cast<uintptr_t>(rhs) | reinterpret_cast<uintptr_t>(sgeo)) & 15) == 0;
     if (kernel == 2 && !(MMA_OK && aligned2)) return cudaErrorNotSupported;
+    if (kernel == 4 && !(LEAN_OK && aligned2)) return cudaErrorNotSupported;
+    // the shape's default; the grouped stage takes no element range and no
+    // test hook, the pipelined one does
+    if (kernel == 0 && DEFAULT_KERNEL == 3) kernel = (probe || ebeg) ? 1 : 3;
     if (ebeg < 0 || ebeg > nelem) return cudaErrorInvalidValue;
     const int64_t groups = (nelem - ebeg + C::EPB - 1) / C::EPB;
     if (groups == 0) return cudaSuccess;
@@ -853,6 +876,21 @@ struct Launch {
         if (g > groups) g = groups;
         const S src{Qin, Qout, rhs, vgeo, sgeo, nbr, D, nelem, qref, rkbdt, status, probe, ebeg};
         k_stage_mma<S, PM::MINB><<<(int)g, PM::THREADS, PM::smem(), st>>>(src, p, rka);
+        return cudaGetLastError();
+      }
+    }
+    if constexpr (LEAN_OK) {
+      if (kernel == 4 || (kernel == 0 && LEAN_DEFAULT && aligned2)) {
+        using S = MeshSrc<T, NS, C::EPB>;
+        using PL = Lean<DIM, Nq, T>;
+        static int per_sm[MAX_DEVICES] = {0};
+        int bps = 0;
+        cudaError_t err = blocks_per_sm(k_stage_lean<DIM, Nq, T, S>, C::THREADS, PL::smem(), per_sm, &bps);
+        if (err != cudaSuccess) return err;
+        int64_t g = (int64_t)num_sms() * bps;
+        if (g > groups) g = groups;
+        const S src{Qin, Qout, rhs, vgeo, sgeo, nbr, D, nelem, qref, rkbdt, status, probe, ebeg};
+        k_stage_lean<DIM, Nq, T, S><<<(int)g, C::THREADS, PL::smem(), st>>>(src, p, rka);
         return cudaGetLastError();
       }
     }
@@ -895,7 +933,7 @@ struct Launch {
   static bool ranged(const void *Qin, const void *rhs, const void *vgeo, const void *sgeo) {
     const bool a = ((reinterpret_cast<uintptr_t>(Qin) | reinterpret_cast<uintptr_t>(rhs) |
                      reinterpret_cast<uintptr_t>(vgeo) | reinterpret_cast<uintptr_t>(sgeo)) & 15) == 0;
-    return a && (Pipe2<DIM, Nq, T>::OK || MMA_OK);
+    return a && (Pipe2<DIM, Nq, T>::OK || MMA_OK || LEAN_OK);
   }
   static cudaError_t build_nbr(int32_t *nbr, const int64_t *vmapM, const int64_t *vmapP,
                                const int64_t *bnd, int64_t nelem, unsigned *status,

@@ -33,6 +33,8 @@ struct Ops {
   bool (*ranged)(const void *, const void *, const void *, const void *);
   bool mma;          // whether the tensor-core stage is built for this shape
   bool mma_default;  // whether it is the shape's default stage kernel
+  bool lean;         // whether the lean pipelined stage is built for this shape
+  int default_kernel;  // the stage kernel choice 0 resolves to (1 to 4)
   cudaError_t (*build_nbr)(int32_t *, const int64_t *, const int64_t *, const int64_t *, int64_t,
                            unsigned *, cudaStream_t);
   // the same with neighbours allowed up to a total element count (ghosts)

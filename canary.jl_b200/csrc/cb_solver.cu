@@ -603,7 +603,12 @@ int cb_solver_set_offset(cb_solver *s, const double *qref) {
 }
 
 int cb_solver_set_kernel(cb_solver *s, int kernel) {
-  if (!s || kernel < 0 || kernel > 3) return solver_fail(CB_ERR_ARG, "cb_solver_set_kernel: bad arguments");
+  if (!s || kernel < 0 || kernel > 4) return solver_fail(CB_ERR_ARG, "cb_solver_set_kernel: bad arguments");
+  if (kernel == 4) {
+    const bool lean = s->prec == 64 ? ops<double>(s)->lean : ops<float>(s)->lean;
+    if (!lean || s->phys.visc > 0)
+      return solver_fail(CB_ERR_UNSUPPORTED, "cb_solver_set_kernel: the lean stage is not built for this shape");
+  }
   if (kernel == 2) {
     const bool mma = s->prec == 64 ? ops<double>(s)->mma : ops<float>(s)->mma;
     if (!mma || s->phys.visc > 0)
@@ -617,8 +622,8 @@ int cb_solver_set_kernel(cb_solver *s, int kernel) {
 
 int cb_solver_get_kernel(const cb_solver *s, int *kernel) {
   if (!s || !kernel) return solver_fail(CB_ERR_ARG, "cb_solver_get_kernel: null argument");
-  const bool mma_def = s->prec == 64 ? ops<double>(s)->mma_default : ops<float>(s)->mma_default;
-  *kernel = s->kernel ? s->kernel : (mma_def && s->phys.visc <= 0 ? 2 : 1);
+  const int def = s->prec == 64 ? ops<double>(s)->default_kernel : ops<float>(s)->default_kernel;
+  *kernel = s->kernel ? s->kernel : (s->phys.visc > 0 ? 1 : def);
   return CB_OK;
 }
 

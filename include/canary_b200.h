@@ -190,10 +190,12 @@ int cb_solver_status_async(cb_solver *s, unsigned *out_host);
  * DMMA tiles, for FP32 solvers on the FP32 fluxes converted to FP64, the sum
  * rounded once; built for 3-D N=7, CB_ERR_UNSUPPORTED elsewhere), 3 = the
  * unpipelined grouped stages (the inviscid k_stage; for the fused viscous
- * form the grouped stage pass instead of the pipelined one).  The default is
- * the fastest on B200 for the shape.  All agree with the oracle to
- * round-off; changing it re-captures the step graph at the next run.
- * cb_solver_get_kernel reports the kernel the solver runs (1, 2 or 3). */
+ * form the grouped passes instead of the pipelined ones), 4 = the lean
+ * pipelined stage of the inviscid form (only the state staged in shared
+ * memory, the geometry and carry read from L2; bit-identical to 1).  The
+ * default is the fastest on B200 for the shape.  All agree with the oracle
+ * to round-off; changing it re-captures the step graph at the next run.
+ * cb_solver_get_kernel reports the kernel the solver runs (1 to 4). */
 int cb_solver_set_kernel(cb_solver *s, int kernel);
 int cb_solver_get_kernel(const cb_solver *s, int *kernel);
 /* Clear the solver's sticky status bits (stream-ordered). */
@@ -351,7 +353,8 @@ int cb_batch_create(cb_batch **out, int precision, int max_instances,
  * two nodes per thread on half the threads; 5 and 9 = the affine-element
  * stage (see cb_batch_set_affine; copies two groups ahead) with one and two
  * nodes per thread; 10 = the tensor-core stage (3-D N=7, as
- * cb_solver_set_kernel 2; the default there for precision 64).  An affine
+ * cb_solver_set_kernel 2; the default there), 11 = the lean pipelined
+ * stage (cb_solver_set_kernel 4).  An affine
  * variant (5, 9) runs on meshes that allow it and falls back to the shape's
  * default per-node variant elsewhere.  A variant
  * chosen here runs as chosen; without a choice the batch uses variant 5 in

@@ -97,8 +97,9 @@ def test_batch_result_same_alone_and_in_mix(cases, precision):
 @pytest.mark.parametrize("precision", [64, 32])
 def test_batch_variants_agree(cases, precision):
     """Grouped variants (1, 2) are bit-identical to each other, and so are the
-    per-node pipelined ones (0, 3, 4, 6, 7, 8: the same code at other
-    occupancies, staging depth, group size or nodes per thread) and the
+    per-node pipelined ones (0, 3, 4, 6, 7, 8, 11: the same code at other
+    occupancies, staging depth, group size or nodes per thread, or with only
+    the state staged) and the
     affine ones (5, 9) on affine meshes; the families sum the contraction
     (padded rows) or form the geometry differently and agree to round-off:
     1e-13 (FP64) / 1e-5 (FP32) relative between the per-node families,

@@ -115,15 +115,17 @@ def test_fp32_tensor_core_stage(n, nsteps, walls):
 @pytest.mark.parametrize("precision,tol", [(64, 1e-12), (32, 1e-5)])
 def test_every_kernel_choice_matches_the_oracle(precision, tol):
     """Kernel choices 0 (default: tensor-core stage), 1 (pipelined CUDA-core
-    stage), 2 (tensor-core) and 3 (unpipelined grouped stage) on one warped
-    3-D N=7 mesh: each against the oracle at the form's bar (FP64 1e-12, FP32
-    1e-5), and the FP64 ones with each other to round-off (1e-13)."""
+    stage), 2 (tensor-core), 3 (unpipelined grouped stage) and 4 (lean
+    pipelined stage: only the state staged) on one warped 3-D N=7 mesh: each
+    against the oracle at the form's bar (FP64 1e-12, FP32 1e-5), the FP64
+    ones with each other to round-off (1e-13), and the lean stage bit for
+    bit with the pipelined CUDA-core one (the same arithmetic)."""
     m, Q, dt = _case(3, seed=5, walls=True)
     ref, rref = Q.copy(order="F"), np.zeros_like(Q, order="F")
     O.lowstorageRK(3, 7, m.vgeo, m.sgeo, ref, rref, m.D, dt, 3, m.vmapM, m.vmapP, m.elemtobndy, _phys(), NT)
     dm = dg.DeviceMesh.upload(m)
     out = {}
-    for kernel in (0, 1, 2, 3):
+    for kernel in (0, 1, 2, 3, 4):
         s = dg.LSRK.for_state(dm, Q, precision)
         s.set_kernel(kernel)
         assert s.kernel == (2 if kernel == 0 else kernel)
@@ -132,15 +134,16 @@ def test_every_kernel_choice_matches_the_oracle(precision, tol):
         s.close()
         assert _relerr(out[kernel], ref) < tol, kernel
     if precision == 64:
-        for kernel in (1, 2, 3):
+        for kernel in (1, 2, 3, 4):
             assert _relerr(out[kernel], out[0]) < 1e-13
+    assert np.array_equal(out[4], out[1])
 
 
 def test_kernel_choice_is_checked():
     m, Q, dt = _case(2)
     dm = dg.DeviceMesh.upload(m)
     s32 = dg.LSRK.for_state(dm, Q, 32)
-    assert s32.kernel in (1, 2)
+    assert s32.kernel == 2
     s32.set_kernel(2)
     assert s32.kernel == 2
     s32.close()
@@ -149,7 +152,7 @@ def test_kernel_choice_is_checked():
     Qv[:, 3] = 1.0
     Qv[:, 4] = 2.5
     s4 = dg.LSRK.for_state(dg.DeviceMesh.upload(mv), Qv, 64)
-    assert s4.kernel == 1
+    assert s4.kernel == 4  # 3-D N=4 FP64 defaults to the lean pipelined stage
     with pytest.raises(CanaryError) as ei:
         s4.set_kernel(2)
     assert ei.value.code == CB_ERR_UNSUPPORTED
