@@ -200,16 +200,14 @@ template <typename T>
 int b_default_var(int dim, int N) {
   // 3-D defaults from the autotuner's B200 timings of one 6 M-node warped
   // instance (ms per step): FP64 N=3 lean 3.03 against 4.11 for variant 0,
-  // N=4 3.46 against 4.46; FP32 N=4 variant 4 1.57 against 1.86, N=5
-  // variant 3 1.34 against 1.39, N=6 variant 8 1.48 against 1.77; N=7 the
-  // tensor-core stage (2.15 / 1.12 against 2.26 / 1.42)
+  // N=4 3.46 against 4.46; N=7 the tensor-core stage (FP64 / FP32 2.15 /
+  // 1.12 against 2.26 / 1.42).  The FP32 3-D orders keep variant 0: their
+  // tuner winners (N=4 variant 4, N=5 variant 3, N=6 variant 8) were timed
+  // on one large instance, while a served stream's 3-D instances are small.
   auto pick = [&](int v) { return b_var_ok<T>(dim, N, v) ? v : -1; };
   int v = -1;
   if (dim == 3 && N == 7 && PipeMT<T>::DEFAULT) v = pick(VAR_MMA);
   else if (dim == 3 && sizeof(T) == 8 && (N == 3 || N == 4)) v = pick(VAR_LEAN);
-  else if (dim == 3 && sizeof(T) == 4 && N == 4) v = pick(4);
-  else if (dim == 3 && sizeof(T) == 4 && N == 5) v = pick(3);
-  else if (dim == 3 && sizeof(T) == 4 && N == 6) v = pick(VAR_NPT2);
   if (v >= 0) return v;
   return b_var_ok<T>(dim, N, 0) ? 0 : b_var_ok<T>(dim, N, 2) ? 2 : 1;
 }
@@ -678,15 +676,17 @@ int cb_mesh_create(cb_mesh **out, int dim, int N, int precision, int64_t nelem, 
   e = o->build_nbr(m->nbr, vmapM, vmapP, elemtobndy, nelem, status, st);
   if (e == cudaSuccess && precision == 32) {
     const int64_t nv = Np * nvg * nelem, nsv = nsg * Nfp * 2 * dim * nelem, nd = (int64_t)Nq * Nq;
-    e = cudaMalloc(&m->owned, sizeof(float) * (nv + nsv + nd));
+    // each array starts on a 16-byte boundary (bulk copies of element slabs)
+    const int64_t nvp = (nv + 3) & ~int64_t(3), nsp = (nsv + 3) & ~int64_t(3);
+    e = cudaMalloc(&m->owned, sizeof(float) * (nvp + nsp + nd));
     if (e == cudaSuccess) {
       float *g = (float *)m->owned;
       if ((e = round_to_f32(g, vgeo, nv, st)) == cudaSuccess &&
-          (e = round_to_f32(g + nv, sgeo, nsv, st)) == cudaSuccess)
-        e = round_to_f32(g + nv + nsv, D, nd, st);
+          (e = round_to_f32(g + nvp, sgeo, nsv, st)) == cudaSuccess)
+        e = round_to_f32(g + nvp + nsp, D, nd, st);
       m->vgeo = g;
-      m->sgeo = g + nv;
-      m->D = g + nv + nsv;
+      m->sgeo = g + nvp;
+      m->D = g + nvp + nsp;
     }
   } else {
     m->vgeo = vgeo;

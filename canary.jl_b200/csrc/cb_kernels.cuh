@@ -856,11 +856,14 @@ struct Launch {
     constexpr bool pipe_ok = Pipe<DIM, Nq, T>::OK;
     const bool aligned = ((reinterpret_cast<uintptr_t>(Qin) | reinterpret_cast<uintptr_t>(vgeo)) & 15) == 0;
     const bool aligned2 = aligned && ((reinterpret_cast<uintptr_t>(rhs) | reinterpret_cast<uintptr_t>(sgeo)) & 15) == 0;
-    if (kernel == 2 && !(MMA_OK && aligned2)) return cudaErrorNotSupported;
-    if (kernel == 4 && !(LEAN_OK && aligned2)) return cudaErrorNotSupported;
     // the shape's default; the grouped stage takes no element range and no
-    // test hook, the pipelined one does
-    if (kernel == 0 && DEFAULT_KERNEL == 3) kernel = (probe || ebeg) ? 1 : 3;
+    // test hook, the pipelined one does (the lean one where the pipelined
+    // plan is not built: ragged FP32 slabs)
+    if (kernel == 0 && DEFAULT_KERNEL == 3)
+      kernel = !(probe || ebeg) ? 3 : (Pipe2<DIM, Nq, T>::OK || !LEAN_OK) ? 1 : 4;
+    if (kernel == 2 && !(MMA_OK && aligned2)) return cudaErrorNotSupported;
+    if (kernel == 4 && !LEAN_OK) return cudaErrorNotSupported;
+    if (kernel == 4 && !aligned2) kernel = 1;  // bulk copies need 16-byte aligned slabs
     if (ebeg < 0 || ebeg > nelem) return cudaErrorInvalidValue;
     const int64_t groups = (nelem - ebeg + C::EPB - 1) / C::EPB;
     if (groups == 0) return cudaSuccess;

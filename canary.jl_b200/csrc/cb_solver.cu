@@ -483,15 +483,18 @@ int solver_create(cb_solver **out, int dim, int N, int precision, int64_t nelem,
     s->D = D;
   } else {
     const int64_t nv = Np * nvg * nelem, ns_ = nsg * Nfp * nface * nelem, nd = (int64_t)Nq * Nq;
-    if ((e = cudaMalloc(&s->owned_geo, sizeof(float) * (nv + ns_ + nd))) != cudaSuccess)
+    // each array starts on a 16-byte boundary (the pipelined stages copy
+    // element slabs with bulk copies)
+    const int64_t nvp = (nv + 3) & ~int64_t(3), nsp = (ns_ + 3) & ~int64_t(3);
+    if ((e = cudaMalloc(&s->owned_geo, sizeof(float) * (nvp + nsp + nd))) != cudaSuccess)
       return bail(CB_ERR_NOMEM, "fp32 geometry");
     float *g = (float *)s->owned_geo;
     round_to_f32(g, vgeo, nv, s->stream);
-    round_to_f32(g + nv, sgeo, ns_, s->stream);
-    round_to_f32(g + nv + ns_, D, nd, s->stream);
+    round_to_f32(g + nvp, sgeo, ns_, s->stream);
+    round_to_f32(g + nvp + nsp, D, nd, s->stream);
     s->vgeo = g;
-    s->sgeo = g + nv;
-    s->D = g + nv + ns_;
+    s->sgeo = g + nvp;
+    s->D = g + nvp + nsp;
   }
   e = precision == 64 ? ops<double>(s)->prepare() : ops<float>(s)->prepare();
   if (e != cudaSuccess) return bail(CB_ERR_CUDA, "kernel attributes");

@@ -59,10 +59,10 @@ def test_parts_equal_single_mesh(case, world, visc, precision, faces):
     parts = [P.GhostedLSRK(m, P.plan(m, r, world), Q, precision, dg.make_phys(**phys), stream=stream)
              for r in range(world)]
     if visc == 0.0:
-        # interior / boundary halves wherever the stage runs over element
-        # ranges: not 3-D N=4 in FP32, whose two-element slabs (1000 bytes)
-        # are not 16-byte multiples and take the unpipelined stage
-        assert all(p.split for p in parts) != (case == "cube4w" and precision == 32)
+        # interior / boundary halves in every shape here: 3-D N=4 in FP32,
+        # whose element slabs (2500 bytes) are not 16-byte multiples, runs
+        # its ranges on the lean stage
+        assert all(p.split for p in parts)
     P.run_parts(parts, k, dt, faces=faces)
     got = np.concatenate([p.state() for p in parts], axis=2)
     for p in parts:
