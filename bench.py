@@ -61,6 +61,10 @@ def bytes_per_node(dim, N, w):
     return w * (4 * ns + (dim * dim + 2) + (2.0 * dim / (N + 1)) * (dim + 1))
 
 
+L2_BYTES = 126e6
+STAGE_KERNELS = {1: "k_stage_pipe2", 2: "k_stage_mma", 3: "k_stage", 4: "k_stage_lean"}
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -447,7 +451,7 @@ def fp32_form(args, dev, stream):
     e1.record(stream)
     torch.cuda.synchronize(dev)
     ms = e0.elapsed_time(e1)
-    kernel = "k_stage_mma" if s.kernel == 2 else "k_stage_pipe2"
+    kernel = STAGE_KERNELS[s.kernel]
     finite = bool(np.all(np.isfinite(s.sums())))
     s.close()
     mesh = dm.mesh
@@ -545,8 +549,9 @@ def main():
     ap.add_argument("--precision", type=int, default=64, choices=[64, 32])
     ap.add_argument("--n-side", type=int, default=32)
     ap.add_argument("--order", type=int, default=7)
-    ap.add_argument("--stage-kernel", type=int, default=0, choices=[0, 1, 2],
-                    help="stage kernel: 0 default, 1 CUDA-core pipelined, 2 tensor-core (3-D N=7 FP64)")
+    ap.add_argument("--stage-kernel", type=int, default=0, choices=[0, 1, 2, 3, 4],
+                    help="stage kernel: 0 the shape's default, 1 CUDA-core pipelined, 2 tensor-core "
+                         "(3-D N=7), 3 grouped, 4 lean pipelined")
     ap.add_argument("--ref-n-side", type=int, default=None,
                     help="mesh of the reference arm (default: --n-side, the same workload)")
     ap.add_argument("--e2e-steps", type=int, default=20)
@@ -591,7 +596,7 @@ def main():
     solver = dg.LSRK(dm, dQ, drhs, args.precision, dg.make_phys(), stream)
     solver.set_offset(off)
     solver.set_kernel(args.stage_kernel)
-    kernel_name = "k_stage_mma" if solver.kernel == 2 else "k_stage_pipe2"
+    kernel_name = STAGE_KERNELS[solver.kernel]
     dof = mesh.nelem * mesh.Np * 5
     dQ0 = dQ.clone()  # initial state, for the parity run
 
@@ -694,6 +699,10 @@ def main():
     peak, peak_kind = measured_peaks()
     achieved = nodes * bpn / t_launch / 1e9
     key = f"{kernel_name}_3d_N{N}_fp{args.precision}_n{args.n_side}"
+    state_gb = dQ.numel() * w / 1e9
+    geo_gb = nodes * (bpn - 4 * 5 * w) / 1e9  # metric and face geometry
+    l2_note = (f"inputs {'larger' if nodes * bpn > L2_BYTES else 'smaller'} than L2 "
+               f"(state {state_gb:.2f} GB, geometry {geo_gb:.2f} GB in FP{args.precision})")
     traffic = load_traffic(key)
     value = world * dof * 5 * args.steps / (t_ms * 1e-3)
     bi = dQ.numel() * w
@@ -707,7 +716,7 @@ def main():
                                "warped x_i += 0.05 sin x sin y sin z, seeded Fourier state (seed 0)",
                    "n_side": args.n_side, "order": N, "nelem": mesh.nelem, "dof": dof, "dt": dt,
                    "parallelism": f"replicas{world}",
-                   "l2": "inputs larger than L2 (state 0.67 GB, geometry 2.4 GB in FP64)",
+                   "l2": l2_note,
                    "state_finite": finite},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,

@@ -256,8 +256,8 @@ int cb_solver_unpack_faces(cb_solver *s, int what, const int64_t *codes, int64_t
  * stage for those elements, half = 1 for the others (once the ghosts of the
  * state the stage reads are filled) and then makes the other buffer
  * current; a stage split this way equals cb_solver_stage bit for bit.
- * Inviscid form, shapes whose stage runs over element ranges (the pipelined
- * and tensor-core stages); CB_ERR_UNSUPPORTED otherwise. */
+ * Inviscid form, shapes whose stage runs over element ranges (the pipelined,
+ * lean and tensor-core stages); CB_ERR_UNSUPPORTED otherwise. */
 int cb_solver_set_split(cb_solver *s, int64_t ninterior);
 int cb_solver_stage_split(cb_solver *s, int stage, double dt, int half, void **next_in);
 
