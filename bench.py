@@ -753,7 +753,11 @@ def main():
                                parity_sample=16 if args.parity_steps > 0 else 0,
                                precisions=tuple(args.batched_precisions), tune=not args.no_autotune)
         if args.precision == 64 and "fp32" in bat:
+            # against the headline FP64 single-mesh stage (3-D, another workload)
             bat["fp32_over_fp64_plain"] = bat["fp32"]["value"] / value
+        if "fp32" in bat and "fp64" in bat:
+            # against the FP64 form of the same ensemble
+            bat["fp32_over_fp64_batched"] = bat["fp32"]["value"] / bat["fp64"]["value"]
         line["batched"] = bat
     if world == 1 and not args.no_served:
         from canary_b200 import serve
