@@ -857,10 +857,12 @@ struct Launch {
     const bool aligned = ((reinterpret_cast<uintptr_t>(Qin) | reinterpret_cast<uintptr_t>(vgeo)) & 15) == 0;
     const bool aligned2 = aligned && ((reinterpret_cast<uintptr_t>(rhs) | reinterpret_cast<uintptr_t>(sgeo)) & 15) == 0;
     // the shape's default; the grouped stage takes no element range and no
-    // test hook, the pipelined one does (the lean one where the pipelined
-    // plan is not built: ragged FP32 slabs)
-    if (kernel == 0 && DEFAULT_KERNEL == 3)
-      kernel = !(probe || ebeg) ? 3 : (Pipe2<DIM, Nq, T>::OK || !LEAN_OK) ? 1 : 4;
+    // test hook: those calls take the pipelined stage, or the lean one where
+    // the pipelined plan does not fit shared memory (3-D N=9 FP64, N=10 FP32)
+    if (kernel == 0 && (probe || ebeg) && (DEFAULT_KERNEL == 1 || DEFAULT_KERNEL == 3))
+      kernel = (Pipe2<DIM, Nq, T>::OK || !LEAN_OK) ? 1 : 4;
+    else if (kernel == 0 && DEFAULT_KERNEL == 3)
+      kernel = 3;
     if (kernel == 2 && !(MMA_OK && aligned2)) return cudaErrorNotSupported;
     if (kernel == 4 && !LEAN_OK) return cudaErrorNotSupported;
     if (kernel == 4 && !aligned2) kernel = 1;  // bulk copies need 16-byte aligned slabs

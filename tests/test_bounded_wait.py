@@ -48,11 +48,11 @@ def _case(dim, N, n):
     return m, np.asfortranarray(Q), dt
 
 
-# 3-D N=7: the tensor-core stage; 2-D N=4: the pipelined one; 3-D N=4: the
-# lean one (the FP64 default, and FP32's stage for the test hook, whose
-# 2500-byte element slabs take no pipelined plan)
+# 3-D N=7: the tensor-core stage; 2-D N=4 and 3-D N=4 FP32: the pipelined
+# one; 3-D N=4 FP64 (its default) and N=9 FP64 (no pipelined plan fits): the
+# lean one
 @pytest.mark.parametrize("dim,N,n,precision", [(3, 7, 6, 64), (3, 7, 4, 32), (2, 4, 12, 64),
-                                               (3, 4, 4, 64), (3, 4, 4, 32)])
+                                               (3, 4, 4, 64), (3, 4, 4, 32), (3, 9, 3, 64)])
 def test_timed_out_wait_stores_nothing_and_reports(dim, N, n, precision):
     import torch
     m, Q, dt = _case(dim, N, n)

@@ -41,14 +41,15 @@ def square(N, n):
 
 @pytest.mark.parametrize("case,world,visc", [("cube3", 2, 0.0), ("cube3", 5, 0.0), ("cube4w", 3, 0.0),
                                              ("square", 4, 0.0), ("cube3", 3, 0.02), ("square", 2, 0.02),
-                                             ("cube7", 2, 0.0)])
+                                             ("cube7", 2, 0.0), ("cube9", 2, 0.0)])
 @pytest.mark.parametrize("precision", [64, 32])
 @pytest.mark.parametrize("faces", [True, False])
 def test_parts_equal_single_mesh(case, world, visc, precision, faces):
     """Inviscid and LDG Navier–Stokes (state and gradient exchanged)."""
     import torch
     m, Q, dt = {"cube3": lambda: cube(3, 4), "cube4w": lambda: cube(4, 3, walls=True),
-                "square": lambda: square(5, 6), "cube7": lambda: cube(7, 3)}[case]()
+                "square": lambda: square(5, 6), "cube7": lambda: cube(7, 3),
+                "cube9": lambda: cube(9, 3)}[case]()
     k = 3
     phys = dict(dg.WORKLOAD_PHYS, visc=visc)
     single = dg.LSRK.for_state(dg.DeviceMesh.upload(m), Q, precision, phys=dg.make_phys(**phys))
@@ -59,15 +60,20 @@ def test_parts_equal_single_mesh(case, world, visc, precision, faces):
     parts = [P.GhostedLSRK(m, P.plan(m, r, world), Q, precision, dg.make_phys(**phys), stream=stream)
              for r in range(world)]
     if visc == 0.0:
-        # interior / boundary halves in every shape here: 3-D N=4 in FP32,
-        # whose element slabs (2500 bytes) are not 16-byte multiples, runs
-        # its ranges on the lean stage
+        # interior / boundary halves in every shape here (3-D N=9 FP64: by
+        # the lean stage, the pipelined plan does not fit shared memory)
         assert all(p.split for p in parts)
     P.run_parts(parts, k, dt, faces=faces)
     got = np.concatenate([p.state() for p in parts], axis=2)
     for p in parts:
         p.close()
-    assert np.array_equal(got, ref)
+    if case == "cube9":
+        # the interior half runs the shape's default stage (grouped), the
+        # boundary half the lean (FP64) or pipelined (FP32) one: the two
+        # agree to rounding, not bit for bit
+        assert max(relerr_fields(got, ref)) < (1e-12 if precision == 64 else 1e-5)
+    else:
+        assert np.array_equal(got, ref)
     if precision == 64 and faces:
         assert max(relerr_fields(got, oracle_run(m, Q, dt, k, phys=phys))) < 1e-12
 
