@@ -839,16 +839,16 @@ struct Launch {
     *out = cache[dev];
     return cudaSuccess;
   }
-  // kernel: 0 = the default for the shape (the tensor-core stage where it is
-  // built, else the pipelined CUDA-core stage, else the older ones), 1 = the
+  // kernel: 0 = the default for the shape (DEFAULT_KERNEL), 1 = the
   // CUDA-core stages only, 2 = the tensor-core stage (cudaErrorNotSupported
   // where it is not built), 3 = the unpipelined grouped stage k_stage, 4 =
-  // the lean pipelined stage k_stage_lean (state-only staging).  probe != 0: the timeout test hook of the
-  // pipelined stages (see MeshSrc); shapes without one return
-  // cudaErrorNotSupported for it.
+  // the lean pipelined stage k_stage_lean (state-only staging; the pipelined
+  // stage where the arrays are not 16-byte aligned).  probe != 0: the timeout
+  // test hook of the pipelined, lean and tensor-core stages (see MeshSrc);
+  // shapes without one return cudaErrorNotSupported for it.
   // ebeg: the launch covers elements ebeg .. nelem - 1 (neighbour indices
-  // stay absolute); only the pipelined and tensor-core stages take ebeg > 0,
-  // the others return cudaErrorNotSupported for it.
+  // stay absolute); only the pipelined, lean and tensor-core stages take
+  // ebeg > 0, the others return cudaErrorNotSupported for it.
   static cudaError_t stage(const T *Qin, T *Qout, T *rhs, const T *vgeo, const T *sgeo,
                            const int32_t *nbr, const T *D, int64_t nelem, const PhysT<T> &p,
                            const Offs<T, NS> &qref, T rka, T rkbdt, unsigned *status,
