@@ -812,8 +812,10 @@ struct Launch {
   // 3.45 / 2.67, N=6 3.37 / 5.13 / 3.83, N=8 5.78 / 5.71 / 5.33; FP32 N=3
   // 1.34 / 1.31 / 1.66, N=4 2.61 / 1.75 / 2.26, N=5 1.65 / 1.44 / 1.72, N=6
   // 2.02 / 1.68 / 2.61, N=8 3.08 / 2.61 / 3.44, N=9 2.22 / 1.93 / 2.45 (the
-  // FP32 pipelined plans fit fewer blocks per SM than the grouped stage).
-  // 3-D N=7 runs the tensor-core stage in both precisions.
+  // FP32 pipelined plans fit fewer blocks per SM than the grouped stage;
+  // FP64 N=8, 9 have no pipelined plan that fits shared memory, so their
+  // first figure is the grouped stage as well).  3-D N=7 runs the
+  // tensor-core stage in both precisions.
   static constexpr int DEFAULT_KERNEL =
       MMA_DEFAULT ? 2
       : DIM == 3 && sizeof(T) == 8 && LEAN_OK && (Nq == 4 || Nq == 5 || Nq == 9) ? 4
